@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Benchmark: single-source BFS (the XBFS hot path) on one or more B200s.
+
+Default workload: Graph500 R-MAT scale 23, edge factor 32 (a=.57 b=.19
+c=.19, symmetrised, deduplicated, seeded), 64 sources drawn uniformly from
+non-isolated vertices; a step is one BFS from one source (sources cycle).
+Metric: GTEPS (Graph500 m_c / time), with the achieved HBM GB/s of the
+traversal kernel in ``roofline``.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+``--impl reference`` times the reference's own CPU BFS (the level-synchronous
+sweep of bfs_gpu_update.cu:105-127, restated in oracle/ and run with all host
+threads) on the same graph and sources. Multi-GPU runs are replicas (every
+rank traverses its own copy of the graph from its own sources; no exchange).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GTEPS + HBM GB/s at R-MAT s23 on 1 B200; batched/learned vs plain; serve p99"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=256)
+    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["rmat", "grid"], default="rmat")
+    ap.add_argument("--scale", type=int, default=23)
+    ap.add_argument("--ef", type=int, default=32)
+    ap.add_argument("--grid-w", type=int, default=4096)
+    ap.add_argument("--grid-h", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--sources", type=int, default=64)
+    ap.add_argument("--policy", default="heuristic")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-flush", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=32)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the cpu_baseline sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {
+        "hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+        "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80, "sync_boost": 0x10,
+    }
+
+    def __init__(self, device: int, period_s: float = 0.02):
+        self.device, self.period = device, period_s
+        self.samples: list[tuple[int, int]] = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((mhz, rs))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.nv:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        mhz = [s[0] for s in self.samples]
+        mask = 0
+        for s in self.samples:
+            mask |= s[1]
+        reasons = [k for k, v in self.REASONS.items() if mask & v]
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def peak_hbm() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(workload_tag: str):
+    """dram bytes per launch of the traversal kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"k_bfs_{workload_tag}.txt")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def allreduce(vals, op):
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=op)
+    return t.tolist()
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def make_graph(args, device):
+    from xbfs_b200 import Graph
+    if args.workload == "rmat":
+        g = Graph.rmat(args.scale, args.ef, args.seed, device=device)
+        name = f"rmat-s{args.scale}-ef{args.ef}"
+    else:
+        g = Graph.grid(args.grid_w, args.grid_h, device=device)
+        name = f"grid-{args.grid_w}x{args.grid_h}"
+    return g, name
+
+
+def cpu_sample(beg, csr, srcs, budget_s):
+    """Serial FIFO BFS (the oracle) on a bounded sample of sources."""
+    import oracle
+    done, edges, t_total = [], 0, 0.0
+    for s in srcs:
+        t0 = time.perf_counter()
+        lv = oracle.bfs_queue(beg, csr, s)
+        t_total += time.perf_counter() - t0
+        edges += oracle.edges_mc(beg, lv)
+        done.append(int(s))
+        if t_total > budget_s:
+            break
+    return edges / t_total / 1e9, done, t_total
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from xbfs_b200 import BfsOptions, pick_sources
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    dev = local
+    g, wname = make_graph(args, dev)
+    V, E = g.V, g.E
+    beg = g.offsets()
+    srcs = pick_sources(beg, args.sources, args.seed + rank)
+    stream = torch.cuda.current_stream()
+    opts = BfsOptions(policy=args.policy, stream=stream.cuda_stream)
+    lv = torch.empty(V, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step(i, timed_events=None):
+        if not args.no_flush:
+            flush.fill_(i & 0xFF)
+        if timed_events is not None:
+            timed_events[0].record(stream)
+        r = g.bfs(int(srcs[i % len(srcs)]), levels=lv, opts=opts)
+        if timed_events is not None:
+            timed_events[1].record(stream)
+        return r
+
+    for i in range(args.warmup):
+        step(i)
+    barrier(world)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    results = []
+    t_wall0 = time.perf_counter()
+    with ClockSampler(dev) as clk:
+        for i in range(args.steps):
+            results.append(step(args.warmup + i, evs[i]))
+        barrier(world)
+    t_wall = time.perf_counter() - t_wall0
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    kernel_ms = [r.kernel_ms for r in results]
+    edges = sum(r.edges_mc for r in results)
+    my_ms = sum(step_ms)
+    if world > 1:
+        tot_edges, = allreduce([float(edges)], dist.ReduceOp.SUM)
+        max_ms, = allreduce([my_ms], dist.ReduceOp.MAX)
+    else:
+        tot_edges, max_ms = float(edges), my_ms
+    value = tot_edges / (max_ms * 1e-3) / 1e9
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_lv = torch.empty(V, dtype=torch.int32, pin_memory=True).numpy()
+        for i in range(2):
+            g.bfs(int(srcs[i % len(srcs)]), levels=host_lv, opts=opts)
+        barrier(world)
+        t0 = time.perf_counter()
+        e_edges = 0
+        for i in range(args.e2e_steps):
+            r = g.bfs(int(srcs[i % len(srcs)]), levels=host_lv, opts=opts)
+            e_edges += r.edges_mc
+        barrier(world)
+        e_s = time.perf_counter() - t0
+        if world > 1:
+            e_edges, = allreduce([float(e_edges)], dist.ReduceOp.SUM)
+            e_s, = allreduce([e_s], dist.ReduceOp.MAX)
+        e2e = {"value": round(e_edges / e_s / 1e9, 3), "unit": "GTEPS",
+               "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * V,
+               "note": "xbfs_bfs with a pinned host level array: D2H of int32[V] levels per step; "
+                       "the source id travels in the launch parameters; graph resident in HBM"}
+
+    # ---- roofline of the traversal kernel
+    b_alg = 8 * (V + 1) + 4 * E + 4 * V
+    mean_k = statistics.mean(kernel_ms)
+    achieved = b_alg / (mean_k * 1e-3) / 1e9
+    peak, peak_kind = peak_hbm()
+    tag = f"rmat_s{args.scale}_ef{args.ef}" if args.workload == "rmat" else f"grid_{args.grid_w}x{args.grid_h}"
+    traffic = ncu_traffic(tag)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "k_bfs (persistent cooperative level loop)",
+                "algorithmic_bytes_per_launch": b_alg,
+                "mean_launch_ms": round(mean_k, 5)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        _, csr = g.download()
+        gteps, done, secs = cpu_sample(beg, csr, srcs, args.cpu_seconds)
+        cpu = {"value": round(gteps, 4), "unit": "GTEPS", "cores": 1, "kind": "port",
+               "sample": f"serial FIFO BFS (oracle) from {len(done)} of the {len(srcs)} sources, {secs:.1f} s"}
+        del csr
+    strat = {"td_queue": 0, "td_scan": 0, "bu": 0}
+    for r in results:
+        for k in strat:
+            strat[k] += r.strategies[k]
+    depth = statistics.median(r.depth for r in results)
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GTEPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded Graph500 R-MAT generated on the device)" if args.workload == "rmat"
+        else "synthetic (2D 4-neighbour grid)",
+        "config": {"workload": f"{wname} single-source BFS", "V": V, "E": E, "sources": len(srcs),
+                   "policy": args.policy, "seed": args.seed,
+                   "l2": "flushed between steps (256 MB write, untimed)" if not args.no_flush else "not flushed",
+                   "parallelism": f"replicas x{world}", "median_depth": depth, "levels_by_strategy": strat},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "clocks": clk.summary(), "gpu_launches": 2 * args.steps,
+        "wall_s_timed_region": round(t_wall, 4),
+        "hbm_gbs_algorithmic_per_step": round(b_alg * args.steps / (max_ms * 1e-3) / 1e9, 1),
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    g.free()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's CPU BFS (sweep, bfs_gpu_update.cu:105-127), all host threads."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    from xbfs_b200 import gen_grid_host, gen_rmat_host, pick_sources
+    threads = len(os.sched_getaffinity(0))
+    try:
+        import torch
+        have_gpu = torch.cuda.is_available()
+    except Exception:
+        have_gpu = False
+    if have_gpu:
+        g, wname = make_graph(args, 0)   # input preparation only; not timed
+        beg, csr = g.download()
+        g.free()
+    elif args.workload == "rmat":
+        beg, csr = gen_rmat_host(args.scale, args.ef, args.seed)
+        wname = f"rmat-s{args.scale}-ef{args.ef}"
+    else:
+        beg, csr = gen_grid_host(args.grid_w, args.grid_h)
+        wname = f"grid-{args.grid_w}x{args.grid_h}"
+    srcs = pick_sources(beg, args.sources, args.seed)
+    for i in range(args.warmup):
+        oracle.bfs_sweep(beg, csr, srcs[i % len(srcs)], threads)
+    t_total, edges = 0.0, 0
+    steps = args.steps
+    budget = 120.0
+    done = 0
+    for i in range(steps):
+        s = srcs[i % len(srcs)]
+        t0 = time.perf_counter()
+        lv, _ = oracle.bfs_sweep(beg, csr, s, threads)
+        t_total += time.perf_counter() - t0
+        edges += oracle.edges_mc(beg, lv)
+        done += 1
+        if t_total > budget:
+            break
+    value = edges / t_total / 1e9
+    out = {
+        "metric": METRIC, "value": round(value, 4), "unit": "GTEPS", "n_gpus": world, "steps": done,
+        "warmup": args.warmup, "ms_per_step": round(t_total / done * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "impl": "reference",
+        "data": "synthetic (seeded Graph500 R-MAT)",
+        "config": {"workload": f"{wname} single-source BFS", "V": len(beg) - 1, "E": int(beg[-1]),
+                   "sources": len(srcs), "seed": args.seed},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": threads, "kind": "port",
+                         "sample": f"reference sweep BFS (bfs_gpu_update.cu:105-127) restated, {done} sources, "
+                                   f"{threads} threads"},
+        "e2e": {"value": round(value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

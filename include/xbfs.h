@@ -1,0 +1,189 @@
+/*
+ * xbfs.h — C ABI of the B200-native XBFS library (libxbfs.so).
+ *
+ * The reference (hpda-lab/XBFS) exposes no library: its interface is the
+ * `bfs` command line (bfs_gpu_update.cu:33-48), the CSR file pair read by
+ * graph.hpp:4-104, and the internal call BFS_ControlFlow<int,long>(...)
+ * (bfs_adaptiveFQ_wb_async.cuh:934-935) that main() makes after allocating
+ * every device buffer itself (bfs_gpu_update.cu:175-251). Each entry point
+ * below names the piece of that interface it replaces.
+ *
+ * Conventions
+ *  - Every call returns an xbfs_status (0 = OK). The library never exits the
+ *    process (the reference's H_ERR calls exit(1), bfs_single_scan.cuh:11-19).
+ *    xbfs_last_error() gives a thread-local detail string for the last failure.
+ *  - Level arrays are int32[V]: source -> 0, BFS depth for reached vertices,
+ *    -1 for unreached (the reference's SA/status contract,
+ *    bfs_gpu_update.cu:105-127, 213-218).
+ *  - Output pointers may be host or device memory; the library detects which.
+ *  - A graph handle owns its device copy of the CSR and the traversal scratch.
+ *    One handle must not be used from two host threads at once.
+ */
+#ifndef XBFS_H_
+#define XBFS_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t xbfs_status;
+enum {
+  XBFS_OK = 0,
+  XBFS_ERR_INVALID_ARG = 1,
+  XBFS_ERR_IO = 2,
+  XBFS_ERR_FORMAT = 3,
+  XBFS_ERR_CUDA = 4,
+  XBFS_ERR_OOM = 5,
+  XBFS_ERR_DEVICE_TIMEOUT = 6, /* a bounded device-side wait expired */
+  XBFS_ERR_UNSUPPORTED = 7,
+  XBFS_ERR_INTERNAL = 8,
+  XBFS_ERR_NO_DEVICE = 9,
+  XBFS_ERR_BUSY = 10,
+  XBFS_ERR_LEVEL_OVERFLOW = 11 /* depth exceeded the packed level width */
+};
+
+/* Per-level strategies (the three classes the direction switch chooses among). */
+enum {
+  XBFS_TD_QUEUE = 0, /* top-down, binned frontier queue built during expansion
+                        (replaces small/medium/large_SA_TD_update,
+                        bfs_adaptiveFQ_wb_async.cuh:50-162, and the in-place
+                        variants bfs_TD_scan_free.cuh:23-135) */
+  XBFS_TD_SCAN = 1,  /* top-down, frontier found by a status sweep
+                        (replaces atomic_FQ_Generator2 + *_SA_TD_update2,
+                        bfs_single_scan.cuh:26-126) */
+  XBFS_BU = 2        /* bottom-up over a ballot-scan queue of unvisited vertices
+                        (replaces ballot_counting/FQ_gen/my_prefixsum/
+                        thread_centric_BU_update, bfs_adaptiveFQ_wb_async.cuh:
+                        189-284, 738-777, prefix_sum1.cuh:13-108) */
+};
+
+/* Direction/strategy policies. */
+enum {
+  XBFS_POLICY_HEURISTIC = 0, /* the reference's switch: ratio = m_f/E < alpha
+                                -> top-down, TD_adaptive / hub_before /
+                                hub_after pick the TD variant
+                                (bfs_adaptiveFQ_wb_async.cuh:946-1078, 1114) */
+  XBFS_POLICY_MLP = 1,       /* learned predictor (xbfs_mlp_set_weights) */
+  XBFS_POLICY_FORCED = 2,    /* xbfs_opts.forced[level] (last entry repeats) */
+  XBFS_POLICY_BEAMER = 3     /* classic alpha/beta direction optimisation */
+};
+
+typedef struct xbfs_opts {
+  int32_t struct_size;  /* = sizeof(xbfs_opts); set by xbfs_opts_init */
+  int32_t policy;       /* XBFS_POLICY_* */
+  float alpha;          /* reference threshold, argv[8] (default 0.1) */
+  int32_t block_dim;    /* reference BlockDim argv[4]; 0 = tuned default */
+  int32_t grid_dim;     /* reference GridDim argv[5]; 0 = all resident CTAs */
+  int32_t async_bu;     /* 1 = bottom-up may write level+2 (reference "async",
+                           bfs_adaptiveFQ_wb_async.cuh:764-770); 0 = off */
+  int32_t small_max;    /* degree bin edges: small <= small_max < medium <=  */
+  int32_t medium_max;   /*   medium_max < large (reference: 32 / 256)        */
+  const int8_t* forced; /* XBFS_POLICY_FORCED: host array of XBFS_TD_* / XBFS_BU */
+  int32_t n_forced;
+  int32_t trace;        /* 1 = record a per-level trace (xbfs_last_trace) */
+  void* stream;         /* cudaStream_t to run on; NULL = the handle's stream */
+  int32_t padding;      /* reference argv[11]; only 1 is meaningful (the
+                           reference is wrong for padding > 1) */
+  float beamer_alpha;   /* XBFS_POLICY_BEAMER: TD->BU when m_f > m_u/alpha (14) */
+  float beamer_beta;    /*                     BU->TD when n_f < V/beta (24)   */
+  int32_t reserved[4];
+} xbfs_opts;
+
+typedef struct xbfs_stats {
+  int32_t struct_size;
+  int32_t depth;      /* number of levels: max level + 1 */
+  int64_t reached;    /* vertices with level >= 0 */
+  int64_t edges_mc;   /* Graph500 m_c: (sum of degrees of reached vertices)/2 */
+  double device_ms;   /* traversal time on the device (CUDA events) */
+  double total_ms;    /* wall time of the whole call, copies included */
+  int32_t n_td_queue; /* levels run with each strategy */
+  int32_t n_td_scan;
+  int32_t n_bu;
+  int32_t n_async;    /* vertices given level+2 by bottom-up */
+  double kernel_ms;   /* the persistent traversal launch alone (CUDA events) */
+} xbfs_stats;
+
+typedef struct xbfs_level_trace {
+  int32_t level;
+  int32_t strategy;
+  int64_t n_f; /* frontier vertices at this level */
+  int64_t m_f; /* frontier edges (sum of degrees) */
+  int64_t n_u; /* unvisited non-isolated vertices */
+  int64_t m_u; /* their edges */
+  double us;   /* device time of this level (globaltimer) */
+} xbfs_level_trace;
+
+typedef struct xbfs_graph xbfs_graph;
+
+const char* xbfs_strerror(xbfs_status st);
+const char* xbfs_last_error(void);
+int32_t xbfs_version(void);
+xbfs_status xbfs_device_count(int32_t* n);
+void xbfs_opts_init(xbfs_opts* o);
+
+/* Load the reference's CSR pair: <beg> = raw little-endian int64[V+1],
+ * <csr> = raw int32[beg[V]]; V = size(beg)/8 - 1. Replaces
+ * graph<int,long,int,int,long,char>::graph (graph.hpp:4-104) — but validates
+ * (monotone offsets, beg[0]=0, in-range neighbours, sizes agree) and returns
+ * XBFS_ERR_FORMAT instead of asserting. */
+xbfs_status xbfs_graph_load(const char* beg_path, const char* csr_path, int32_t device,
+                            xbfs_graph** out);
+/* Upload a host CSR (same layout). Replaces the cudaMalloc/cudaMemcpy of
+ * beg_cu/csr_cu in main (bfs_gpu_update.cu:175-180). */
+xbfs_status xbfs_graph_upload(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E,
+                              int32_t device, xbfs_graph** out);
+xbfs_status xbfs_graph_info(const xbfs_graph* g, int64_t* V, int64_t* E, int64_t* max_degree,
+                            int64_t* n_isolated);
+/* Copy the device CSR back to host buffers (beg: V+1, csr: E entries; csr
+ * may be NULL to fetch the offsets only). */
+xbfs_status xbfs_graph_download(const xbfs_graph* g, int64_t* beg, int32_t* csr);
+/* Write the handle's CSR in the reference's file format. */
+xbfs_status xbfs_graph_save(const xbfs_graph* g, const char* beg_path, const char* csr_path);
+void xbfs_graph_free(xbfs_graph* g);
+
+/* Single-source BFS. Replaces BFS_ControlFlow<int,long>(...)
+ * (bfs_adaptiveFQ_wb_async.cuh:934-1258) plus the status copy-back in main
+ * (bfs_gpu_update.cu:255). levels: V entries (host or device). parents:
+ * nullable, V entries; parents[src] = src, -1 when unreached. opts, stats:
+ * nullable. The whole level loop runs on the device (one persistent
+ * cooperative launch); no per-level host round trip. */
+xbfs_status xbfs_bfs(xbfs_graph* g, int32_t src, int32_t* levels, int32_t* parents,
+                     const xbfs_opts* opts, xbfs_stats* stats);
+
+/* Per-level trace of the last xbfs_bfs call made with opts.trace = 1
+ * (replaces the reference's tag[]/ratio[]/iter[] arrays, written to
+ * Hybrid_iteration.csv at bfs_gpu_update.cu:270-272). */
+xbfs_status xbfs_last_trace(xbfs_graph* g, xbfs_level_trace* out, int32_t cap, int32_t* n);
+
+/* Synthetic inputs (no reference counterpart: the reference reads datasets
+ * converted by CSRGenerator/tuple_text_to_bin.cpp). All generators are
+ * deterministic functions of their arguments; the host and device builds
+ * produce identical CSRs. Graphs are symmetric, self-loop free, deduplicated,
+ * adjacency sorted ascending. */
+xbfs_status xbfs_gen_rmat(int32_t scale, int32_t edge_factor, uint64_t seed, double a, double b,
+                          double c, int32_t device, xbfs_graph** out);
+xbfs_status xbfs_gen_grid(int32_t width, int32_t height, int32_t device, xbfs_graph** out);
+xbfs_status xbfs_gen_er(int64_t n, double mean_degree, uint64_t seed, int32_t device,
+                        xbfs_graph** out);
+/* Host-only generation (no GPU needed): returns malloc'd arrays that the
+ * caller releases with xbfs_free_host. */
+xbfs_status xbfs_gen_rmat_host(int32_t scale, int32_t edge_factor, uint64_t seed, double a,
+                               double b, double c, int64_t** beg, int32_t** csr, int64_t* V,
+                               int64_t* E);
+xbfs_status xbfs_gen_grid_host(int32_t width, int32_t height, int64_t** beg, int32_t** csr,
+                               int64_t* V, int64_t* E);
+xbfs_status xbfs_gen_er_host(int64_t n, double mean_degree, uint64_t seed, int64_t** beg,
+                             int32_t** csr, int64_t* V, int64_t* E);
+void xbfs_free_host(void* p);
+/* Deterministic source sampling: k sources uniform over vertices with
+ * degree > 0 (host CSR offsets). */
+xbfs_status xbfs_pick_sources(const int64_t* beg, int64_t V, int32_t k, uint64_t seed,
+                              int32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XBFS_H_ */

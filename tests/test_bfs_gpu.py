@@ -1,0 +1,183 @@
+"""Single-source BFS on the GPU through the C ABI, bit-exact against the CPU
+oracle (serial FIFO BFS), on hand graphs, R-MAT, grids and ER graphs, under
+every policy, forced strategy schedules, bin thresholds and with parents
+checked as a BFS tree."""
+import itertools
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.conftest import hand_graphs
+from xbfs_b200 import BfsOptions, Graph, XbfsError, gen_er_host, gen_grid_host, gen_rmat_host, pick_sources
+from xbfs_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def run_and_check(g, beg, csr, src, **kw):
+    want_parents = kw.pop("want_parents", True)
+    r = g.bfs(int(src), want_parents=want_parents, **kw)
+    ref = oracle.bfs_queue(beg, csr, src)
+    assert np.array_equal(r.levels, ref), f"levels differ at {np.nonzero(r.levels != ref)[0][:10]}"
+    if want_parents:
+        assert oracle.check_tree(beg, csr, src, r.levels, r.parents) == 0
+    assert r.depth == int(ref.max()) + 1
+    assert r.reached == int((ref >= 0).sum())
+    assert r.edges_mc == oracle.edges_mc(beg, ref)
+    return r
+
+
+def test_hand_graphs_all_sources():
+    for name, (beg, csr) in hand_graphs().items():
+        g = Graph.from_csr(beg, csr)
+        n = len(beg) - 1
+        for src in range(n) if n <= 40 else [0, 1, n // 2, n - 1]:
+            for policy in ("heuristic", "beamer"):
+                run_and_check(g, beg, csr, src, policy=policy)
+        g.free()
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(10, 16, 1), (12, 8, 2), (14, 16, 3), (16, 16, 4)])
+def test_rmat_heuristic_and_beamer(scale, ef, seed):
+    beg, csr = gen_rmat_host(scale, ef, seed)
+    g = Graph.from_csr(beg, csr)
+    for s in pick_sources(beg, 8, seed):
+        run_and_check(g, beg, csr, s, policy="heuristic")
+        run_and_check(g, beg, csr, s, policy="beamer", want_parents=False)
+        run_and_check(g, beg, csr, s, policy="heuristic", async_bu=False, want_parents=False)
+
+
+def test_every_forced_schedule_prefix_gives_identical_levels():
+    beg, csr = gen_rmat_host(12, 16, 9)
+    g = Graph.from_csr(beg, csr)
+    srcs = pick_sources(beg, 2, 9)
+    for sched in itertools.product(["td_queue", "td_scan", "bu"], repeat=4):
+        for tail in ("td_queue", "td_scan", "bu"):
+            for s in srcs:
+                run_and_check(g, beg, csr, s, policy="forced", forced=list(sched) + [tail],
+                              want_parents=(tail == "bu"))
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_schedules_larger(seed):
+    rng = np.random.default_rng(seed)
+    beg, csr = gen_rmat_host(16, 16, 100 + seed)
+    g = Graph.from_csr(beg, csr)
+    for s in pick_sources(beg, 4, seed):
+        sched = rng.integers(0, 3, size=12).tolist()
+        run_and_check(g, beg, csr, s, policy="forced", forced=sched, async_bu=bool(seed % 2))
+
+
+@pytest.mark.parametrize("small_max,medium_max", [(1, 1), (4, 16), (32, 256), (64, 64), (1024, 4096)])
+def test_bin_thresholds(small_max, medium_max):
+    beg, csr = gen_rmat_host(14, 32, 5)
+    g = Graph.from_csr(beg, csr)
+    for s in pick_sources(beg, 4, 5):
+        run_and_check(g, beg, csr, s, small_max=small_max, medium_max=medium_max,
+                      policy="forced", forced=["td_queue"])
+        run_and_check(g, beg, csr, s, small_max=small_max, medium_max=medium_max)
+
+
+def test_grid_long_diameter():
+    for W, H in [(64, 64), (300, 7), (1, 500), (257, 129)]:
+        beg, csr = gen_grid_host(W, H)
+        g = Graph.from_csr(beg, csr)
+        for s in [0, (W * H) // 2, W * H - 1]:
+            run_and_check(g, beg, csr, s)
+            run_and_check(g, beg, csr, s, policy="forced", forced=["td_scan", "bu", "td_queue"],
+                          want_parents=False)
+
+
+def test_er_and_small_grid_count():
+    beg, csr = gen_er_host(20000, 8.0, 4)
+    g = Graph.from_csr(beg, csr)
+    for s in pick_sources(beg, 6, 4):
+        run_and_check(g, beg, csr, s)
+
+
+def test_asymmetric_graph_never_uses_bottom_up():
+    graphs = hand_graphs()
+    beg, csr = graphs["directed_chain"]
+    g = Graph.from_csr(beg, csr)
+    r = run_and_check(g, beg, csr, 0, policy="forced", forced=["bu"])
+    assert r.strategies["bu"] == 0
+
+
+def test_device_generators_match_host():
+    for args in [(10, 16, 3), (13, 8, 4)]:
+        b, c = gen_rmat_host(*args)
+        g = Graph.rmat(*args)
+        gb, gc = g.download()
+        assert np.array_equal(gb, b) and np.array_equal(gc, c)
+    b, c = gen_grid_host(37, 19)
+    gb, gc = Graph.grid(37, 19).download()
+    assert np.array_equal(gb, b) and np.array_equal(gc, c)
+    b, c = gen_er_host(4000, 8.0, 2)
+    gb, gc = Graph.er(4000, 8.0, 2).download()
+    assert np.array_equal(gb, b) and np.array_equal(gc, c)
+
+
+def test_device_output_buffers_and_reuse():
+    import torch
+    beg, csr = gen_rmat_host(13, 16, 8)
+    g = Graph.from_csr(beg, csr)
+    lv = torch.empty(g.V, dtype=torch.int32, device="cuda:0")
+    pa = torch.empty(g.V, dtype=torch.int32, device="cuda:0")
+    for s in pick_sources(beg, 5, 8):
+        g.bfs(int(s), levels=lv, parents=pa)
+        torch.cuda.synchronize()
+        ref = oracle.bfs_queue(beg, csr, s)
+        assert np.array_equal(lv.cpu().numpy(), ref)
+        assert oracle.check_tree(beg, csr, s, ref, pa.cpu().numpy()) == 0
+
+
+def test_heuristic_trace_matches_reference_schedule():
+    beg, csr = gen_rmat_host(16, 16, 21)
+    g = Graph.from_csr(beg, csr)
+    for s in pick_sources(beg, 6, 21):
+        r = g.bfs(int(s), trace=True)
+        ref = oracle.bfs_queue(beg, csr, s)
+        tags = oracle.reference_schedule(beg, ref, 0.1)
+        mine = [t["strategy"] for t in r.trace][: len(tags)]
+        expect = ["bu" if t == -1 else ("td_scan" if t == 1 else "td_queue") for t in tags]
+        assert mine == expect
+        assert all(t["us"] >= 0 for t in r.trace)
+        assert [t["n_f"] for t in r.trace] == [int((ref == L).sum()) for L in range(len(r.trace))]
+
+
+def test_invalid_arguments():
+    beg, csr = gen_rmat_host(8, 4, 1)
+    g = Graph.from_csr(beg, csr)
+    with pytest.raises(XbfsError) as e:
+        g.bfs(g.V)
+    assert e.value.status == _lib.XBFS_ERR_INVALID_ARG
+    with pytest.raises(XbfsError) as e:
+        g.bfs(0, padding=2)
+    assert e.value.status == _lib.XBFS_ERR_INVALID_ARG
+    with pytest.raises(XbfsError):
+        g.bfs(0, policy="forced", forced=[])
+
+
+def test_load_file_pair_and_malformed_inputs(tmp_path):
+    from xbfs_b200 import write_csr
+    beg, csr = gen_rmat_host(11, 8, 6)
+    write_csr(beg, csr, str(tmp_path / "g_beg_pos.bin"), str(tmp_path / "g_csr.bin"))
+    g = Graph.load(str(tmp_path / "g_beg_pos.bin"), str(tmp_path / "g_csr.bin"))
+    assert g.V == len(beg) - 1 and g.E == len(csr)
+    s = int(pick_sources(beg, 1, 6)[0])
+    run_and_check(g, beg, csr, s)
+    # non-monotone offsets
+    bad = beg.copy()
+    bad[5], bad[6] = bad[6] + 1, bad[5]
+    write_csr(bad, csr, str(tmp_path / "b_beg.bin"), str(tmp_path / "b_csr.bin"))
+    with pytest.raises(XbfsError) as e:
+        Graph.load(str(tmp_path / "b_beg.bin"), str(tmp_path / "b_csr.bin"))
+    assert e.value.status == _lib.XBFS_ERR_FORMAT
+    # out-of-range neighbour
+    badc = csr.copy()
+    badc[7] = len(beg) + 5
+    write_csr(beg, badc, str(tmp_path / "c_beg.bin"), str(tmp_path / "c_csr.bin"))
+    with pytest.raises(XbfsError) as e:
+        Graph.load(str(tmp_path / "c_beg.bin"), str(tmp_path / "c_csr.bin"))
+    assert e.value.status == _lib.XBFS_ERR_FORMAT

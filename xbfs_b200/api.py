@@ -1,0 +1,269 @@
+"""Python host API over libxbfs.so.
+
+Mirrors the reference's interface for the BFS path:
+
+* the CSR file pair of graph.hpp:4-104 (``Graph.load``),
+* the parameters of the reference's command line / BFS_ControlFlow
+  (bfs_gpu_update.cu:33-48, bfs_adaptiveFQ_wb_async.cuh:934-935):
+  ``alpha``, ``block_dim``, ``grid_dim``, ``padding``, source vertex,
+* the per-vertex int32 level array (-1 = unreached) it produces
+  (bfs_gpu_update.cu:213-218, 255).
+
+Errors are raised as :class:`XbfsError` carrying the library status code.
+Outputs are numpy arrays (host) or, when a CUDA tensor is passed, written in
+place on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import BU, TD_QUEUE, TD_SCAN, LevelTrace, Opts, Stats, XbfsError, check, lib
+
+POLICIES = {"heuristic": _lib.POLICY_HEURISTIC, "mlp": _lib.POLICY_MLP,
+            "forced": _lib.POLICY_FORCED, "beamer": _lib.POLICY_BEAMER}
+STRATEGIES = {"td_queue": TD_QUEUE, "td_scan": TD_SCAN, "bu": BU}
+
+RMAT_A, RMAT_B, RMAT_C = 0.57, 0.19, 0.19  # Graph500 Kronecker parameters
+
+
+def _ptr(a) -> int:
+    """Data pointer of a numpy array or torch tensor (host or device)."""
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())
+
+
+@dataclass
+class BfsOptions:
+    """Per-call options (xbfs_opts). ``policy``: heuristic | mlp | forced | beamer."""
+    policy: str = "heuristic"
+    alpha: float = 0.1
+    block_dim: int = 0
+    grid_dim: int = 0
+    async_bu: bool = True
+    small_max: int = 32
+    medium_max: int = 256
+    forced: Optional[Sequence[int]] = None
+    trace: bool = False
+    padding: int = 1
+    beamer_alpha: float = 14.0
+    beamer_beta: float = 24.0
+    stream: int = 0
+    _keep: list = field(default_factory=list, repr=False)
+
+    def to_c(self) -> Opts:
+        o = Opts()
+        lib.xbfs_opts_init(C.byref(o))
+        o.policy = POLICIES[self.policy] if isinstance(self.policy, str) else int(self.policy)
+        o.alpha = float(self.alpha)
+        o.block_dim = int(self.block_dim)
+        o.grid_dim = int(self.grid_dim)
+        o.async_bu = 1 if self.async_bu else 0
+        o.small_max = int(self.small_max)
+        o.medium_max = int(self.medium_max)
+        o.trace = 1 if self.trace else 0
+        o.padding = int(self.padding)
+        o.beamer_alpha = float(self.beamer_alpha)
+        o.beamer_beta = float(self.beamer_beta)
+        o.stream = self.stream or None
+        if self.forced is not None:
+            vals = [STRATEGIES[s] if isinstance(s, str) else int(s) for s in self.forced]
+            arr = (C.c_int8 * max(1, len(vals)))(*vals)
+            self._keep = [arr]
+            o.forced = C.cast(arr, C.POINTER(C.c_int8))
+            o.n_forced = len(vals)
+        return o
+
+
+@dataclass
+class BfsResult:
+    levels: object
+    parents: object
+    depth: int
+    reached: int
+    edges_mc: int
+    device_ms: float
+    total_ms: float
+    kernel_ms: float
+    strategies: dict
+    n_async: int
+    trace: Optional[list] = None
+
+    @property
+    def gteps(self) -> float:
+        return self.edges_mc / (self.device_ms * 1e-3) / 1e9 if self.device_ms > 0 else 0.0
+
+
+class Graph:
+    """A CSR graph resident on one GPU (xbfs_graph handle)."""
+
+    def __init__(self, handle: int, device: int):
+        self._h = C.c_void_p(handle)
+        self.device = device
+        V, E, md, ni = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib.xbfs_graph_info(self._h, C.byref(V), C.byref(E), C.byref(md), C.byref(ni)))
+        self.V, self.E, self.max_degree, self.n_isolated = V.value, E.value, md.value, ni.value
+
+    # -- construction ------------------------------------------------------
+    @classmethod
+    def load(cls, beg_path: str, csr_path: str, device: int = 0) -> "Graph":
+        h = C.c_void_p()
+        check(lib.xbfs_graph_load(beg_path.encode(), csr_path.encode(), device, C.byref(h)))
+        return cls(h.value, device)
+
+    @classmethod
+    def from_csr(cls, beg: np.ndarray, csr: np.ndarray, device: int = 0) -> "Graph":
+        beg = np.ascontiguousarray(beg, dtype=np.int64)
+        csr = np.ascontiguousarray(csr, dtype=np.int32)
+        h = C.c_void_p()
+        check(lib.xbfs_graph_upload(beg.ctypes.data, csr.ctypes.data if csr.size else None,
+                                    len(beg) - 1, len(csr), device, C.byref(h)))
+        return cls(h.value, device)
+
+    @classmethod
+    def rmat(cls, scale: int, edge_factor: int, seed: int = 1, a: float = RMAT_A, b: float = RMAT_B,
+             c: float = RMAT_C, device: int = 0) -> "Graph":
+        h = C.c_void_p()
+        check(lib.xbfs_gen_rmat(scale, edge_factor, seed, a, b, c, device, C.byref(h)))
+        return cls(h.value, device)
+
+    @classmethod
+    def grid(cls, width: int, height: int, device: int = 0) -> "Graph":
+        h = C.c_void_p()
+        check(lib.xbfs_gen_grid(width, height, device, C.byref(h)))
+        return cls(h.value, device)
+
+    @classmethod
+    def er(cls, n: int, mean_degree: float = 8.0, seed: int = 1, device: int = 0) -> "Graph":
+        h = C.c_void_p()
+        check(lib.xbfs_gen_er(n, mean_degree, seed, device, C.byref(h)))
+        return cls(h.value, device)
+
+    # -- lifetime ------------------------------------------------------------
+    def free(self) -> None:
+        if self._h:
+            lib.xbfs_graph_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- data ------------------------------------------------------------------
+    def offsets(self) -> np.ndarray:
+        beg = np.empty(self.V + 1, dtype=np.int64)
+        check(lib.xbfs_graph_download(self._h, beg.ctypes.data, None))
+        return beg
+
+    def download(self) -> tuple[np.ndarray, np.ndarray]:
+        beg = np.empty(self.V + 1, dtype=np.int64)
+        csr = np.empty(max(self.E, 1), dtype=np.int32)
+        check(lib.xbfs_graph_download(self._h, beg.ctypes.data, csr.ctypes.data))
+        return beg, csr[: self.E]
+
+    def save(self, beg_path: str, csr_path: str) -> None:
+        check(lib.xbfs_graph_save(self._h, beg_path.encode(), csr_path.encode()))
+
+    # -- traversal -------------------------------------------------------------
+    def bfs(self, src: int, levels=None, parents=None, want_parents: bool = False,
+            opts: Optional[BfsOptions] = None, **kw) -> BfsResult:
+        """Single-source BFS. ``levels``/``parents`` may be preallocated numpy
+        arrays or CUDA tensors of V int32; otherwise numpy arrays are returned."""
+        if opts is None:
+            opts = BfsOptions(**kw)
+        elif kw:
+            raise TypeError("pass either opts or keyword options")
+        if levels is None:
+            levels = np.empty(self.V, dtype=np.int32)
+        if parents is None and want_parents:
+            parents = np.empty(self.V, dtype=np.int32)
+        o = opts.to_c()
+        st = Stats()
+        st.struct_size = C.sizeof(Stats)
+        check(lib.xbfs_bfs(self._h, int(src), _ptr(levels), _ptr(parents) if parents is not None else None,
+                           C.byref(o), C.byref(st)))
+        trace = self.last_trace() if opts.trace else None
+        return BfsResult(levels=levels, parents=parents, depth=st.depth, reached=st.reached,
+                         edges_mc=st.edges_mc, device_ms=st.device_ms, total_ms=st.total_ms,
+                         kernel_ms=st.kernel_ms,
+                         strategies={"td_queue": st.n_td_queue, "td_scan": st.n_td_scan, "bu": st.n_bu},
+                         n_async=st.n_async, trace=trace)
+
+    def last_trace(self) -> list[dict]:
+        n = C.c_int32(0)
+        check(lib.xbfs_last_trace(self._h, None, 0, C.byref(n)))
+        buf = (LevelTrace * max(1, n.value))()
+        check(lib.xbfs_last_trace(self._h, buf, n.value, C.byref(n)))
+        return [{"level": t.level, "strategy": _lib.STRATEGY_NAMES.get(t.strategy, t.strategy),
+                 "n_f": t.n_f, "m_f": t.m_f, "n_u": t.n_u, "m_u": t.m_u, "us": t.us}
+                for t in buf[: n.value]]
+
+
+# ---------------------------------------------------------------------------
+# Host-side generators (no GPU needed); identical output to the device ones.
+# ---------------------------------------------------------------------------
+def _take_host(pb, pc, V, E) -> tuple[np.ndarray, np.ndarray]:
+    beg = np.ctypeslib.as_array(pb, shape=(V.value + 1,)).copy()
+    csr = np.ctypeslib.as_array(pc, shape=(max(E.value, 1),))[: E.value].copy()
+    lib.xbfs_free_host(C.cast(pb, C.c_void_p))
+    lib.xbfs_free_host(C.cast(pc, C.c_void_p))
+    return beg, csr
+
+
+def gen_rmat_host(scale: int, edge_factor: int, seed: int = 1, a: float = RMAT_A, b: float = RMAT_B,
+                  c: float = RMAT_C) -> tuple[np.ndarray, np.ndarray]:
+    pb, pc = C.POINTER(C.c_int64)(), C.POINTER(C.c_int32)()
+    V, E = C.c_int64(), C.c_int64()
+    check(lib.xbfs_gen_rmat_host(scale, edge_factor, seed, a, b, c, C.byref(pb), C.byref(pc),
+                                 C.byref(V), C.byref(E)))
+    return _take_host(pb, pc, V, E)
+
+
+def gen_grid_host(width: int, height: int) -> tuple[np.ndarray, np.ndarray]:
+    pb, pc = C.POINTER(C.c_int64)(), C.POINTER(C.c_int32)()
+    V, E = C.c_int64(), C.c_int64()
+    check(lib.xbfs_gen_grid_host(width, height, C.byref(pb), C.byref(pc), C.byref(V), C.byref(E)))
+    return _take_host(pb, pc, V, E)
+
+
+def gen_er_host(n: int, mean_degree: float = 8.0, seed: int = 1) -> tuple[np.ndarray, np.ndarray]:
+    pb, pc = C.POINTER(C.c_int64)(), C.POINTER(C.c_int32)()
+    V, E = C.c_int64(), C.c_int64()
+    check(lib.xbfs_gen_er_host(n, mean_degree, seed, C.byref(pb), C.byref(pc), C.byref(V), C.byref(E)))
+    return _take_host(pb, pc, V, E)
+
+
+def pick_sources(beg: np.ndarray, k: int, seed: int = 1) -> np.ndarray:
+    beg = np.ascontiguousarray(beg, dtype=np.int64)
+    out = np.empty(max(k, 1), dtype=np.int32)
+    check(lib.xbfs_pick_sources(beg.ctypes.data, len(beg) - 1, k, seed, out.ctypes.data))
+    return out[:k]
+
+
+def write_csr(beg: np.ndarray, csr: np.ndarray, beg_path: str, csr_path: str) -> None:
+    """Write the reference's file pair: raw int64 beg_pos, raw int32 csr."""
+    np.ascontiguousarray(beg, dtype="<i8").tofile(beg_path)
+    np.ascontiguousarray(csr, dtype="<i4").tofile(csr_path)
+
+
+def read_csr(beg_path: str, csr_path: str) -> tuple[np.ndarray, np.ndarray]:
+    beg = np.fromfile(beg_path, dtype="<i8")
+    csr = np.fromfile(csr_path, dtype="<i4")
+    return beg, csr[: int(beg[-1])]

@@ -1,0 +1,1023 @@
+// Single-source direction-optimising BFS on B200: one persistent cooperative
+// launch runs the whole level loop on the device.
+//
+// Reference path replaced (hpda-lab/XBFS):
+//   BFS_ControlFlow            bfs_adaptiveFQ_wb_async.cuh:934-1258  (host level loop)
+//   small/medium/large_SA_TD_update   bfs_adaptiveFQ_wb_async.cuh:50-162
+//   small/medium/large_SA_TD_update1  bfs_TD_scan_free.cuh:23-135
+//   atomic_FQ_Generator2 + *_SA_TD_update2   bfs_single_scan.cuh:26-126
+//   ballot_counting, FQ_gen    bfs_adaptiveFQ_wb_async.cuh:189-284
+//   my_prefixsum / IntraBlockSum / InterBlockSum   prefix_sum1.cuh:13-108
+//   thread_centric_BU_update   bfs_adaptiveFQ_wb_async.cuh:738-777
+//   swap (queue ping-pong)     swap.cuh:10-15
+//   switch heuristic           bfs_adaptiveFQ_wb_async.cuh:946-958, 1042-1078, 1114
+//
+// Design (B200-first, not a translation):
+//  * The reference returns to the host every level: it sums frontier edges
+//    with an O(V) host loop, copies the whole status array back, and checks
+//    termination against the CPU answer. Here the level loop, the statistics
+//    (n_f, m_f, n_u, m_u, reduced inside the kernels) and the strategy
+//    decision live on the device; levels are separated by a bounded grid
+//    barrier (~1-2 us) instead of a host round trip.
+//  * Status is kept twice: the int32 level array (the output contract) and
+//    bitmaps - visited (pre-seeded with isolated vertices), and a ring of four
+//    frontier bitmaps (level L, L+1, L+2 for the asynchronous bottom-up, and
+//    one being cleared). At scale 23 each bitmap is 1 MB, so every random
+//    status probe hits L2 (126 MB), while the CSR is streamed with an
+//    evict-first hint.
+//  * Frontier queues are degree-binned (small / medium / large, thresholds
+//    tunable, reference 32 / 256) and carry an exclusive edge offset per
+//    entry, reserved with one packed 64-bit atomic (count | edges). Expansion
+//    is edge-balanced: each CTA takes an equal slice of each bin's edge space
+//    and walks its owners with a shared-memory window, so a hub vertex with
+//    10^5 neighbours is spread over the whole GPU instead of one CTA.
+//  * Winners are staged per CTA in shared memory and flushed with one global
+//    atomic per bin per flush instead of one atomicAdd per vertex.
+//  * Bottom-up builds a ballot/popcount-compacted, sorted list of unvisited
+//    vertices per CTA (the reference's ballot_counting + prefix sum + FQ_gen,
+//    without the host round trip of my_prefixsum), then warps drain it with
+//    early exit and the reference's asynchronous level+2 rule.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace xbfs {
+
+constexpr int kBlock = 512;         // threads per CTA of the traversal kernel
+constexpr int kK = 2;               // edges per thread per gather round
+constexpr int kTE = kBlock * kK;    // edges per gather round
+constexpr int kCap = 2048;          // staging capacity, small and medium bins
+constexpr int kCapL = 512;          // staging capacity, large bin
+constexpr int kFlushAt = kCap - kTE;
+constexpr int kFlushAtL = kCapL / 2;  // large-bin overflow goes straight to the global queue
+
+constexpr unsigned long long kCountMask = (1ull << 31) - 1;
+
+struct FDesc {
+  unsigned long long bin[3];  // packed: (edges << 31) | count
+  unsigned long long n;       // vertices in the frontier (degree-0 included)
+  unsigned long long m;       // sum of their degrees
+  unsigned long long pend_n;  // part found early by asynchronous bottom-up
+  unsigned long long pend_m;
+  unsigned long long pad;
+};
+
+struct LevelRecDev {
+  int strategy;
+  int flags;
+  long long n_f, m_f, n_u, m_u;
+  unsigned long long t0, t1;
+};
+
+struct Ctl {
+  GridBarrier bar;
+  int err;
+  int depth;
+  unsigned long long n_async;   // vertices given level+2 by bottom-up
+  unsigned long long reached;   // sum of frontier sizes
+  unsigned long long msum;      // sum of frontier degrees
+  int strat_count[4];
+  FDesc fd[4];
+};
+
+struct MlpWeights;  // mlp.cu
+
+struct Params {
+  const long long* beg;
+  const int* csr;
+  long long V, E;
+  int* levels;
+  int* parents;
+  uint32_t* vis;
+  uint32_t* fb[4];
+  int* qids[2][3];
+  unsigned* qeb[2][3];
+  int* ulist;
+  Ctl* ctl;
+  LevelRecDev* hist;
+  int hist_cap;
+  const signed char* forced;
+  int n_forced;
+  long long nwords;  // bitmap words covering V
+  long long n_ni;    // non-isolated vertices
+  int policy;
+  float alpha;
+  int async_bu;
+  int small_max, medium_max;
+  float beamer_alpha, beamer_beta;
+  unsigned long long timeout_ns;
+  long long max_levels;
+  const float* mlp;  // packed MLP weights (may be null)
+  int allow_bu;      // 0 when the CSR is not symmetric: bottom-up would miss parents
+};
+
+// ---------------------------------------------------------------------------
+// Shared memory layout of the traversal kernel (dynamic).
+// ---------------------------------------------------------------------------
+struct __align__(16) Smem {
+  long long wbeg[kTE + 1];
+  unsigned web[kTE + 1];
+  int wu[kTE + 1];
+  int st_id[2][kCap];
+  int st_deg[2][kCap];
+  int stl_id[kCapL];
+  int stl_deg[kCapL];
+  int cnt[3];
+  int strategy;
+  int next_s;
+  int bu_next;
+  int bu_n;
+  int flag;
+  unsigned long long base_slot, base_edge;
+  long long red[kBlock / 32 + 1];
+  float mlp_h[2][32];
+  int go;
+};
+
+__device__ __forceinline__ int bin_of(long long d, int small_max, int medium_max) {
+  return d <= small_max ? 0 : (d <= medium_max ? 1 : 2);
+}
+
+// ---------------------------------------------------------------------------
+// Strategy policy (computed identically by thread 0 of every CTA).
+// ---------------------------------------------------------------------------
+struct PolicyState {
+  // reference heuristic state (bfs_adaptiveFQ_wb_async.cuh:946-1078)
+  long long count_prev;
+  int is_change;
+  long long td_adaptive;
+  long long hub_before;
+  long long hub_after;
+  int tag_prev;  // 0: scan-free / last-phase TD, 1: second-phase TD, -1: BU
+  // Beamer
+  int bu_dir;
+  // features
+  long long n_prev;
+  int prev_strategy;
+};
+
+constexpr long long kInfinite = 10000;  // bfs_adaptiveFQ_wb_async.cuh:29
+
+// The reference's switch restated on device statistics. The reference
+// computes count[level] = sum of degrees of status==level vertices with a host
+// sweep (cuh:1042-1046); here that number is m_f, reduced inside the kernels.
+__device__ int decide_reference(PolicyState& ps, long long L, long long m_f, long long E, float alpha) {
+  const long long cnt = m_f;
+  if (!ps.is_change) {
+    if (L == 0 && cnt >= kInfinite) {
+      ps.is_change = 1;
+      ps.td_adaptive = L + 1;
+    } else if (L > 0 && ps.count_prev >= kInfinite && cnt >= kInfinite * 10 &&
+               cnt / ps.count_prev >= 8) {
+      ps.is_change = 1;
+      ps.td_adaptive = L;
+    } else if ((L > 0 && cnt >= kInfinite * 100) ||
+               (L > 0 && ps.count_prev < kInfinite && cnt >= kInfinite * 10 && ps.count_prev > 0 &&
+                cnt / ps.count_prev >= 1000)) {
+      ps.is_change = 1;
+      ps.td_adaptive = L;
+    }
+  }
+  const float ratio = (float)cnt / (float)(E > 0 ? E : 1);
+  if (ratio >= alpha && ps.tag_prev >= 0) ps.hub_before = L;
+  if (ratio < alpha && ps.tag_prev == -1) ps.hub_after = L;
+  int s;
+  if (ratio < alpha) {
+    if (ps.hub_before == 0 && L < ps.td_adaptive) {
+      s = XBFS_TD_QUEUE;  // scan-free top-down (cuh:1078-1110)
+      ps.tag_prev = 0;
+    } else if (ps.hub_after > 0 && L > ps.hub_after) {
+      s = XBFS_TD_QUEUE;  // "last phase" top-down (cuh:1114-1125)
+      ps.tag_prev = 0;
+    } else {
+      s = XBFS_TD_SCAN;   // "second phase" single-scan top-down (cuh:1128-1153)
+      ps.tag_prev = 1;
+    }
+  } else {
+    s = XBFS_BU;
+    ps.tag_prev = -1;
+  }
+  ps.count_prev = cnt;
+  return s;
+}
+
+__device__ int decide_beamer(PolicyState& ps, long long n_f, long long m_f, long long m_u, long long V,
+                             float a, float b) {
+  if (!ps.bu_dir) {
+    if ((double)m_f > (double)m_u / (double)a) ps.bu_dir = 1;
+  } else {
+    if ((double)n_f < (double)V / (double)b) ps.bu_dir = 0;
+  }
+  return ps.bu_dir ? XBFS_BU : XBFS_TD_QUEUE;
+}
+
+// MLP inference (8 -> 32 -> 32 -> 3), one warp, weights packed as
+// [mean 8][std 8][W1 32x8][b1 32][W2 32x32][b2 32][W3 3x32][b3 3].
+__device__ int mlp_decide(const float* w, const float feat[8], float* h1s, float* h2s, int lane) {
+  const float* mean = w;
+  const float* sd = w + 8;
+  const float* W1 = w + 16;
+  const float* B1 = W1 + 256;
+  const float* W2 = B1 + 32;
+  const float* B2 = W2 + 1024;
+  const float* W3 = B2 + 32;
+  const float* B3 = W3 + 96;
+  float x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) x[i] = (feat[i] - mean[i]) / sd[i];
+  float a = B1[lane];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) a = fmaf(W1[lane * 8 + i], x[i], a);
+  a = fmaxf(a, 0.f);
+  h1s[lane] = a;
+  __syncwarp();
+  float b = B2[lane];
+  for (int i = 0; i < 32; ++i) b = fmaf(W2[lane * 32 + i], h1s[i], b);
+  b = fmaxf(b, 0.f);
+  h2s[lane] = b;
+  __syncwarp();
+  float o[3];
+  for (int k = 0; k < 3; ++k) {
+    float t = W3[k * 32 + lane] * b;
+    t = warp_sum(t);
+    o[k] = t + B3[k];
+  }
+  int best = 0;
+  if (o[1] > o[best]) best = 1;
+  if (o[2] > o[best]) best = 2;
+  return best;
+}
+
+__device__ __forceinline__ float flog(double x) { return (float)log1p(x > 0 ? x : 0.0); }
+
+// ---------------------------------------------------------------------------
+// Staging of top-down winners (per CTA) and flush to the global binned queue.
+// ---------------------------------------------------------------------------
+struct QOut {
+  int* ids[3];
+  unsigned* eb[3];
+  unsigned long long* ctr;  // fd[..].bin
+};
+
+__device__ __forceinline__ void direct_enqueue(const QOut& q, int bin, int v, long long d) {
+  unsigned long long old = atomicAdd(&q.ctr[bin], ((unsigned long long)d << 31) | 1ull);
+  unsigned long long slot = old & kCountMask;
+  q.ids[bin][slot] = v;
+  q.eb[bin][slot] = (unsigned)(old >> 31);
+}
+
+__device__ __forceinline__ void stage(Smem& sm, const QOut& q, int bin, int v, long long d) {
+  int slot = atomicAdd(&sm.cnt[bin], 1);
+  if (bin < 2) {
+    if (slot < kCap) {
+      sm.st_id[bin][slot] = v;
+      sm.st_deg[bin][slot] = (int)d;
+      return;
+    }
+  } else if (slot < kCapL) {
+    sm.stl_id[slot] = v;
+    sm.stl_deg[slot] = (int)d;
+    return;
+  }
+  direct_enqueue(q, bin, v, d);
+}
+
+// Block-wide flush of all staged winners (call from all threads, uniform).
+__device__ void flush(Smem& sm, const QOut& q) {
+  __syncthreads();
+  for (int bin = 0; bin < 3; ++bin) {
+    const int cap = bin < 2 ? kCap : kCapL;
+    int n = sm.cnt[bin];
+    if (n > cap) n = cap;
+    if (n == 0) continue;
+    int* ids = bin < 2 ? sm.st_id[bin] : sm.stl_id;
+    int* degs = bin < 2 ? sm.st_deg[bin] : sm.stl_deg;
+    // each thread owns a contiguous run of PER items
+    constexpr int PER = (kCap + kBlock - 1) / kBlock;
+    const int i0 = threadIdx.x * PER;
+    long long loc = 0;
+    for (int k = 0; k < PER; ++k)
+      if (i0 + k < n) loc += degs[i0 + k];
+    long long total;
+    long long ex = block_exclusive_scan<kBlock, long long>(loc, sm.red, &total);
+    if (threadIdx.x == 0) {
+      unsigned long long old = atomicAdd(&q.ctr[bin], ((unsigned long long)total << 31) | (unsigned long long)n);
+      sm.base_slot = old & kCountMask;
+      sm.base_edge = old >> 31;
+    }
+    __syncthreads();
+    const unsigned long long bs = sm.base_slot, be = sm.base_edge;
+    long long run = ex;
+    for (int k = 0; k < PER; ++k) {
+      int i = i0 + k;
+      if (i < n) {
+        q.ids[bin][bs + i] = ids[i];
+        q.eb[bin][bs + i] = (unsigned)(be + run);
+        run += degs[i];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sm.cnt[bin] = 0;
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ bool need_flush(const Smem& sm) {
+  return sm.cnt[0] >= kFlushAt || sm.cnt[1] >= kFlushAt || sm.cnt[2] >= kFlushAtL;
+}
+
+// ---------------------------------------------------------------------------
+// Per-thread statistics for the frontier being produced.
+// ---------------------------------------------------------------------------
+struct Acc {
+  long long n1, m1;  // level+1 winners
+  long long n2, m2;  // level+2 (asynchronous bottom-up)
+};
+
+template <bool PAR>
+__device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& q, Acc& acc, int v, int u,
+                                         int L, bool enq, uint32_t* fbn) {
+  const uint32_t word = (uint32_t)v >> 5, bit = 1u << (v & 31);
+  if (ld_cg_u32(p.vis + word) & bit) return;
+  const uint32_t old = atomicOr(p.vis + word, bit);
+  if (old & bit) return;
+  p.levels[v] = L + 1;
+  if (PAR) p.parents[v] = u;
+  const long long d = ld_nc_i64(p.beg + v + 1) - ld_nc_i64(p.beg + v);
+  acc.n1 += 1;
+  acc.m1 += d;
+  if (enq) {
+    if (d > 0) stage(sm, q, bin_of(d, p.small_max, p.medium_max), v, d);
+  } else {
+    red_or_u32(fbn + word, bit);
+  }
+}
+
+// Warp 0 finds the last slot s in [0, cnt) with eb[s] <= key (eb strictly
+// increasing, eb[0] == 0 <= key). 32-ary search.
+__device__ int find_owner(const unsigned* eb, unsigned cnt, unsigned long long key) {
+  const int lane = threadIdx.x & 31;
+  unsigned lo = 0, hi = cnt;  // answer in [lo, hi)
+  while (hi - lo > 32) {
+    const unsigned span = hi - lo;
+    const unsigned piv = lo + (unsigned)(((unsigned long long)span * lane) / 32);
+    const bool le = (unsigned long long)eb[piv] <= key;
+    const unsigned mask = __ballot_sync(0xffffffffu, le);
+    const int last = 31 - __clz(mask);  // lane 0 always true (eb[lo] <= key)
+    const unsigned nlo = lo + (unsigned)(((unsigned long long)span * last) / 32);
+    const unsigned nhi = (last == 31) ? hi : lo + (unsigned)(((unsigned long long)span * (last + 1)) / 32);
+    lo = nlo;
+    hi = nhi;
+  }
+  const unsigned idx = lo + lane;
+  const bool le = idx < hi && (unsigned long long)eb[idx] <= key;
+  const unsigned mask = __ballot_sync(0xffffffffu, le);
+  return (int)(lo + 31 - __clz(mask));
+}
+
+// Edge-balanced expansion of one bin of the current frontier queue.
+template <bool PAR>
+__device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, const int* ids,
+                           const unsigned* eb, unsigned cnt, unsigned long long M, int L, bool enq,
+                           uint32_t* fbn) {
+  if (cnt == 0 || M == 0) return;
+  const unsigned long long G = gridDim.x, b = blockIdx.x;
+  const unsigned long long lo = M * b / G, hi = M * (b + 1) / G;
+  if (lo >= hi) return;
+  if (threadIdx.x < 32) {
+    int s = find_owner(eb, cnt, lo);
+    if (threadIdx.x == 0) sm.next_s = s;
+  }
+  __syncthreads();
+  unsigned s = (unsigned)sm.next_s;
+  for (unsigned long long r = lo; r < hi; r += kTE) {
+    const unsigned long long rhi = (r + kTE < hi) ? r + kTE : hi;
+    for (int i = threadIdx.x; i <= kTE; i += kBlock) {
+      const unsigned slot = s + (unsigned)i;
+      unsigned e0 = 0xffffffffu;
+      if (slot < cnt) {
+        const unsigned x = eb[slot];
+        if ((unsigned long long)x < rhi) {
+          e0 = x;
+          const int u = ids[slot];
+          sm.wu[i] = u;
+          sm.wbeg[i] = ld_nc_i64(p.beg + u);
+        }
+      }
+      sm.web[i] = e0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+      const unsigned long long e = r + threadIdx.x + (unsigned long long)k * kBlock;
+      if (e < rhi) {
+        // owner: last i with web[i] <= e
+        int a = 0, c = kTE + 1;
+        while (c - a > 1) {
+          const int mid = (a + c) >> 1;
+          if ((unsigned long long)sm.web[mid] <= e) a = mid; else c = mid;
+        }
+        const int u = sm.wu[a];
+        const long long idx = sm.wbeg[a] + (long long)(e - sm.web[a]);
+        const int v = ld_stream_i32(p.csr + idx);
+        claim_td<PAR>(p, sm, q, acc, v, u, L, enq, fbn);
+      }
+    }
+    if (threadIdx.x == 0 && rhi < hi) {
+      int a = 0, c = kTE + 1;
+      while (c - a > 1) {
+        const int mid = (a + c) >> 1;
+        if ((unsigned long long)sm.web[mid] <= rhi) a = mid; else c = mid;
+      }
+      sm.next_s = (int)(s + a);
+    }
+    __syncthreads();
+    s = (unsigned)sm.next_s;
+    if (enq && need_flush(sm)) flush(sm, q);
+  }
+}
+
+// Bitmap of frontier L -> binned queue of frontier L (degree-0 vertices are
+// never queued, as in the reference's bins). Ballot-free: each thread owns one
+// word and emits its set bits one per sub-round so a sub-round stages at most
+// kBlock entries.
+__device__ void sweep_bitmap_to_queue(const Params& p, Smem& sm, const QOut& q, const uint32_t* fbc) {
+  const long long nw = p.nwords;
+  const long long ntile = (nw + kBlock - 1) / kBlock;
+  for (long long t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const long long w = t * kBlock + threadIdx.x;
+    uint32_t bits = (w < nw) ? ld_cg_u32(fbc + w) : 0u;
+    while (__syncthreads_or(bits != 0)) {
+      if (bits) {
+        const int bpos = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const int v = (int)(w * 32 + bpos);
+        const long long d = ld_nc_i64(p.beg + v + 1) - ld_nc_i64(p.beg + v);
+        if (d > 0) stage(sm, q, bin_of(d, p.small_max, p.medium_max), v, d);
+      }
+      __syncthreads();
+      if (need_flush(sm)) flush(sm, q);
+    }
+  }
+  flush(sm, q);
+}
+
+// Queue of frontier L -> bitmap of frontier L.
+__device__ void scatter_queue_to_bitmap(const Params& p, int par, const FDesc& fd, uint32_t* fbc) {
+  const long long tid = blockIdx.x * (long long)kBlock + threadIdx.x;
+  const long long nth = (long long)gridDim.x * kBlock;
+  for (int bin = 0; bin < 3; ++bin) {
+    const long long cnt = (long long)(ld_cg_u64(&fd.bin[bin]) & kCountMask);
+    const int* ids = p.qids[par][bin];
+    for (long long i = tid; i < cnt; i += nth) {
+      const int v = ids[i];
+      red_or_u32(fbc + (v >> 5), 1u << (v & 31));
+    }
+  }
+}
+
+// Bottom-up step for level L over this CTA's slice of the vertex range.
+template <bool PAR, bool ASYNC>
+__device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
+                          uint32_t* fbn2) {
+  const long long nw = p.nwords;
+  const long long G = gridDim.x, b = blockIdx.x;
+  const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
+  int* list = p.ulist + w0 * 32;
+  // 1. ballot/popcount compaction of unvisited vertices into a sorted list
+  long long pos = 0;
+  for (long long wb = w0; wb < w1; wb += kBlock) {
+    const long long w = wb + threadIdx.x;
+    uint32_t bits = (w < w1) ? ~ld_cg_u32(p.vis + w) : 0u;
+    long long total;
+    const long long ex = block_exclusive_scan<kBlock, long long>((long long)__popc(bits), sm.red, &total);
+    long long o = pos + ex;
+    while (bits) {
+      const int bp = __ffs(bits) - 1;
+      bits &= bits - 1;
+      list[o++] = (int)(w * 32 + bp);
+    }
+    pos += total;
+  }
+  if (threadIdx.x == 0) {
+    sm.bu_next = 0;
+    sm.bu_n = (int)pos;
+  }
+  __syncthreads();
+  const int n = sm.bu_n;
+  const int lane = threadIdx.x & 31;
+  // 2. warps drain the list 32 entries at a time
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&sm.bu_next, 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const int i = base + lane;
+    if (i < n) {
+      const int v = list[i];
+      const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
+      int found = -1, found2 = -1;
+      for (long long e = e0; e < e1; e += 4) {
+        int u[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) u[k] = (e + k < e1) ? ld_stream_i32(p.csr + e + k) : -1;
+        uint32_t wc[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) wc[k] = (u[k] >= 0) ? fbc[u[k] >> 5] : 0u;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (found < 0 && u[k] >= 0 && ((wc[k] >> (u[k] & 31)) & 1u)) found = u[k];
+        if (found >= 0) break;
+        if (ASYNC && found2 < 0) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (found2 < 0 && u[k] >= 0 && ((ld_cg_u32(fbn + (u[k] >> 5)) >> (u[k] & 31)) & 1u)) found2 = u[k];
+        }
+      }
+      const uint32_t word = (uint32_t)v >> 5, bit = 1u << (v & 31);
+      if (found >= 0) {
+        p.levels[v] = L + 1;
+        if (PAR) p.parents[v] = found;
+        red_or_u32(p.vis + word, bit);
+        red_or_u32(fbn + word, bit);
+        acc.n1 += 1;
+        acc.m1 += e1 - e0;
+      } else if (ASYNC && found2 >= 0) {
+        p.levels[v] = L + 2;
+        if (PAR) p.parents[v] = found2;
+        red_or_u32(p.vis + word, bit);
+        red_or_u32(fbn2 + word, bit);
+        acc.n2 += 1;
+        acc.m2 += e1 - e0;
+      }
+    }
+  }
+}
+
+// Block-reduce the accumulators and publish them to the frontier descriptors.
+__device__ void publish_acc(Smem& sm, Acc& acc, FDesc* f1, FDesc* f2) {
+  long long n1 = block_sum<kBlock, long long>(acc.n1, sm.red);
+  long long m1 = block_sum<kBlock, long long>(acc.m1, sm.red);
+  long long n2 = 0, m2 = 0;
+  if (f2) {
+    n2 = block_sum<kBlock, long long>(acc.n2, sm.red);
+    m2 = block_sum<kBlock, long long>(acc.m2, sm.red);
+  }
+  if (threadIdx.x == 0) {
+    if (n1) atomicAdd(&f1->n, (unsigned long long)n1);
+    if (m1) atomicAdd(&f1->m, (unsigned long long)m1);
+    if (f2 && n2) {
+      atomicAdd(&f2->n, (unsigned long long)n2);
+      atomicAdd(&f2->m, (unsigned long long)m2);
+      atomicAdd(&f2->pend_n, (unsigned long long)n2);
+      atomicAdd(&f2->pend_m, (unsigned long long)m2);
+    }
+  }
+  acc = Acc{0, 0, 0, 0};
+}
+
+// Distributed clear of a bitmap (each CTA its slice).
+__device__ void clear_bitmap(uint32_t* bm, long long nw) {
+  const long long G = gridDim.x, b = blockIdx.x;
+  const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
+  for (long long w = w0 + threadIdx.x; w < w1; w += kBlock) bm[w] = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// The persistent traversal kernel.
+// ---------------------------------------------------------------------------
+template <bool PAR>
+__global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+  Ctl* ctl = p.ctl;
+  if (threadIdx.x < 3) sm.cnt[threadIdx.x] = 0;
+  __syncthreads();
+
+  PolicyState ps;
+  ps.count_prev = 0;
+  ps.is_change = 0;
+  ps.td_adaptive = kInfinite;
+  ps.hub_before = 0;
+  ps.hub_after = 0;
+  ps.tag_prev = 0;
+  ps.bu_dir = 0;
+  ps.n_prev = 1;
+  ps.prev_strategy = XBFS_TD_QUEUE;
+  long long vis_n = 0, vis_m = 0;  // sum over frontiers <= L (thread 0)
+
+  bool q_valid = true, b_valid = true;
+  unsigned dirty = 1u;  // fb[i] may contain set bits
+  Acc acc{0, 0, 0, 0};
+  const uint32_t nb = gridDim.x;
+  long long L = 0;
+  for (;; ++L) {
+    if (L >= p.max_levels) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctl->err, 0, (int)XBFS_ERR_INTERNAL);
+      break;
+    }
+    FDesc* F0 = &ctl->fd[L & 3];
+    FDesc* F1 = &ctl->fd[(L + 1) & 3];
+    FDesc* F2 = &ctl->fd[(L + 2) & 3];
+    FDesc* F3 = &ctl->fd[(L + 3) & 3];
+    if (threadIdx.x == 0) {
+      const long long n_f = (long long)ld_cg_u64(&F0->n);
+      const long long m_f = (long long)ld_cg_u64(&F0->m);
+      int s = -1;
+      if (n_f > 0) {
+        vis_n += n_f;
+        vis_m += m_f;
+        const long long pn = (long long)ld_cg_u64(&F1->pend_n);
+        const long long pm = (long long)ld_cg_u64(&F1->pend_m);
+        long long n_u = p.n_ni - vis_n - pn;
+        long long m_u = p.E - vis_m - pm;
+        if (n_u < 0) n_u = 0;
+        if (m_u < 0) m_u = 0;
+        switch (p.policy) {
+          case XBFS_POLICY_FORCED: {
+            long long i = L < p.n_forced ? L : p.n_forced - 1;
+            s = (i >= 0) ? (int)p.forced[i] : XBFS_TD_QUEUE;
+            if (s < 0 || s > 2) s = XBFS_TD_QUEUE;
+            break;
+          }
+          case XBFS_POLICY_BEAMER:
+            s = decide_beamer(ps, n_f, m_f, m_u, p.V, p.beamer_alpha, p.beamer_beta);
+            break;
+          case XBFS_POLICY_MLP:
+            s = -2;  // decided by warp 0 below
+            break;
+          default:
+            s = decide_reference(ps, L, m_f, p.E, p.alpha);
+        }
+        if (s == XBFS_BU && !p.allow_bu) s = XBFS_TD_QUEUE;
+        if (s == -2) {
+          // features are stored for warp 0
+          sm.mlp_h[0][0] = flog((double)n_f);
+          sm.mlp_h[0][1] = flog((double)m_f);
+          sm.mlp_h[0][2] = flog((double)n_u);
+          sm.mlp_h[0][3] = flog((double)m_u);
+          sm.mlp_h[0][4] = flog((double)L);
+          sm.mlp_h[0][5] = (float)ps.prev_strategy;
+          sm.mlp_h[0][6] = (float)(log((double)n_f + 1.0) - log((double)ps.n_prev + 1.0));
+          sm.mlp_h[0][7] = flog((double)m_f / (double)n_f);
+        }
+        if (blockIdx.x == 0 && L < p.hist_cap) {
+          LevelRecDev& r = p.hist[L];
+          r.n_f = n_f;
+          r.m_f = m_f;
+          r.n_u = n_u;
+          r.m_u = m_u;
+          r.t0 = globaltimer_ns();
+          r.t1 = 0;
+          if (L > 0 && L - 1 < p.hist_cap) p.hist[L - 1].t1 = r.t0;
+        }
+        ps.n_prev = n_f;
+      }
+      sm.strategy = s;
+    }
+    __syncthreads();
+    if (sm.strategy == -2) {
+      if (threadIdx.x < 32) {
+        float feat[8];
+        for (int i = 0; i < 8; ++i) feat[i] = sm.mlp_h[0][i];
+        __syncwarp();
+        int s = p.mlp ? mlp_decide(p.mlp, feat, sm.mlp_h[0], sm.mlp_h[1], threadIdx.x) : XBFS_TD_QUEUE;
+        if (s == XBFS_BU && !p.allow_bu) s = XBFS_TD_QUEUE;
+        if (threadIdx.x == 0) sm.strategy = s;
+      }
+      __syncthreads();
+    }
+    const int S = sm.strategy;
+    if (S < 0) break;  // empty frontier: done
+    if (threadIdx.x == 0) {
+      ps.prev_strategy = S;
+      if (blockIdx.x == 0) {
+        if (L < p.hist_cap) p.hist[L].strategy = S;
+        ctl->strat_count[S] += 1;
+        ctl->reached += ld_cg_u64(&F0->n);
+        ctl->msum += ld_cg_u64(&F0->m);
+        ctl->n_async += ld_cg_u64(&F0->pend_n);
+      }
+    }
+    // ---- housekeeping for slots no longer in use (first phase of the level)
+    if (blockIdx.x == 0 && threadIdx.x < 8) {
+      reinterpret_cast<unsigned long long*>(F3)[threadIdx.x] = 0ull;
+    }
+    const int c3 = (int)((L + 3) & 3);
+    if (dirty & (1u << c3)) {
+      clear_bitmap(p.fb[c3], p.nwords);
+      dirty &= ~(1u << c3);
+    }
+    uint32_t* fbc = p.fb[L & 3];
+    uint32_t* fbn = p.fb[(L + 1) & 3];
+    uint32_t* fbn2 = p.fb[(L + 2) & 3];
+    const int par = (int)(L & 1);
+
+    if (S == XBFS_TD_QUEUE || S == XBFS_TD_SCAN) {
+      if (!q_valid) {
+        QOut qs;
+        for (int b2 = 0; b2 < 3; ++b2) {
+          qs.ids[b2] = p.qids[par][b2];
+          qs.eb[b2] = p.qeb[par][b2];
+        }
+        qs.ctr = F0->bin;
+        sweep_bitmap_to_queue(p, sm, qs, fbc);
+        if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
+      }
+      const bool enq = (S == XBFS_TD_QUEUE) && (ld_cg_u64(&F1->pend_n) == 0);
+      QOut qo;
+      for (int b2 = 0; b2 < 3; ++b2) {
+        qo.ids[b2] = p.qids[par ^ 1][b2];
+        qo.eb[b2] = p.qeb[par ^ 1][b2];
+      }
+      qo.ctr = F1->bin;
+      for (int bin = 2; bin >= 0; --bin) {
+        const unsigned long long pk = ld_cg_u64(&F0->bin[bin]);
+        gather_bin<PAR>(p, sm, qo, acc, p.qids[par][bin], p.qeb[par][bin], (unsigned)(pk & kCountMask),
+                        pk >> 31, (int)L, enq, fbn);
+      }
+      if (enq) flush(sm, qo);
+      publish_acc(sm, acc, F1, nullptr);
+      if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
+      q_valid = enq;
+      b_valid = !enq;
+      if (!enq) dirty |= 1u << ((L + 1) & 3);
+    } else {
+      if (!b_valid) {
+        scatter_queue_to_bitmap(p, par, *F0, fbc);
+        dirty |= 1u << (L & 3);
+        if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
+      }
+      if (p.async_bu)
+        bottom_up<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+      else
+        bottom_up<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+      publish_acc(sm, acc, F1, F2);
+      if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
+      q_valid = false;
+      b_valid = true;
+      dirty |= 1u << ((L + 1) & 3);
+      if (p.async_bu) dirty |= 1u << ((L + 2) & 3);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl->depth = (int)L;
+    if (L > 0 && L - 1 < p.hist_cap) p.hist[L - 1].t1 = globaltimer_ns();
+  }
+}
+
+// Seeds the traversal: level/parent of the source, its bits, queue entry and
+// frontier descriptor for level 0.
+__global__ void k_seed(Params p, int src, int par_enabled) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  p.levels[src] = 0;
+  if (par_enabled) p.parents[src] = src;
+  const uint32_t word = (uint32_t)src >> 5, bit = 1u << (src & 31);
+  p.vis[word] |= bit;
+  p.fb[0][word] |= bit;
+  const long long d = p.beg[src + 1] - p.beg[src];
+  FDesc& f = p.ctl->fd[0];
+  f.n = 1;
+  f.m = (unsigned long long)d;
+  if (d > 0) {
+    const int bin = bin_of(d, p.small_max, p.medium_max);
+    p.qids[0][bin][0] = src;
+    p.qeb[0][bin][0] = 0;
+    f.bin[bin] = ((unsigned long long)d << 31) | 1ull;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host driver
+// ---------------------------------------------------------------------------
+static xbfs_status ensure_workspace(Graph* g, int small_max, int medium_max) {
+  SsWorkspace& w = g->ss;
+  xbfs_status st;
+  const long long nwords = (g->V + 31) / 32 + 64;
+  if (!w.ready) {
+    w.V = g->V;
+    w.nwords = (size_t)nwords;
+    if ((st = w.bits.ensure((size_t)nwords * 4 * 5))) return st;
+    if ((st = w.ulist.ensure((size_t)nwords * 32 * 4))) return st;
+    if ((st = w.ctl.ensure(sizeof(Ctl)))) return st;
+    w.hist_cap = 1 << 16;
+    if ((st = w.hist.ensure(sizeof(LevelRecDev) * (size_t)w.hist_cap))) return st;
+    XBFS_CUDA_TRY(cudaEventCreate(&w.ev0));
+    XBFS_CUDA_TRY(cudaEventCreate(&w.ev1));
+    XBFS_CUDA_TRY(cudaEventCreate(&w.evk0));
+    w.ready = true;
+  }
+  // queue capacities per bin: vertices with degree in the bin's range
+  auto count_gt = [&](long long t) -> size_t {
+    // vertices with degree > t, upper bound from the power-of-two histogram
+    if (t < 1) return (size_t)g->V;
+    int k = 0;
+    while (k < 15 && (1ll << (k + 1)) <= t) ++k;
+    return (size_t)g->cnt_deg_gt[k];
+  };
+  size_t cap[3];
+  cap[0] = (size_t)g->V;
+  cap[1] = std::min<size_t>((size_t)g->V, count_gt(small_max));
+  cap[2] = std::min<size_t>((size_t)g->V, count_gt(medium_max));
+  for (int b = 0; b < 3; ++b) {
+    if (cap[b] + 1 > w.qcap[b] || !w.qids[0][b].p) {
+      for (int par = 0; par < 2; ++par) {
+        if ((st = w.qids[par][b].ensure((cap[b] + 1) * 4))) return st;
+        if ((st = w.qeb[par][b].ensure((cap[b] + 1) * 4))) return st;
+      }
+      w.qcap[b] = cap[b] + 1;
+    }
+  }
+  return XBFS_OK;
+}
+
+xbfs_status bfs_single(Graph* g, int32_t src, int32_t* levels, int32_t* parents, const xbfs_opts* uopts,
+                       xbfs_stats* stats) {
+  const auto t_start = std::chrono::steady_clock::now();
+  xbfs_opts o;
+  xbfs_opts_init(&o);
+  if (uopts) {
+    if (uopts->struct_size != (int32_t)sizeof(xbfs_opts))
+      return set_error(XBFS_ERR_INVALID_ARG, "xbfs_opts.struct_size = %d, expected %zu (call xbfs_opts_init)",
+                       uopts->struct_size, sizeof(xbfs_opts));
+    o = *uopts;
+  }
+  if (!g) return set_error(XBFS_ERR_INVALID_ARG, "graph is NULL");
+  if (!levels) return set_error(XBFS_ERR_INVALID_ARG, "levels is NULL");
+  if (src < 0 || (int64_t)src >= g->V)
+    return set_error(XBFS_ERR_INVALID_ARG, "source %d out of range [0, %lld)", src, (long long)g->V);
+  if (g->E >= (1ll << 32))
+    return set_error(XBFS_ERR_UNSUPPORTED, "single-source path needs E < 2^32 (E = %lld)", (long long)g->E);
+  if (o.padding != 1)
+    return set_error(XBFS_ERR_INVALID_ARG,
+                     "padding = %d: only 1 is supported (the reference's bottom-up is incorrect for "
+                     "padding > 1)", o.padding);
+  if (o.small_max <= 0) o.small_max = 32;
+  if (o.medium_max < o.small_max) o.medium_max = o.small_max;
+  if (o.policy == XBFS_POLICY_FORCED && (!o.forced || o.n_forced <= 0))
+    return set_error(XBFS_ERR_INVALID_ARG, "forced policy needs a non-empty forced[] array");
+  if (o.policy < 0 || o.policy > 3) return set_error(XBFS_ERR_INVALID_ARG, "bad policy %d", o.policy);
+  if (!(o.alpha > 0)) o.alpha = 0.1f;
+
+  DeviceGuard dg(g->device);
+  xbfs_status st = ensure_workspace(g, o.small_max, o.medium_max);
+  if (st) return st;
+  SsWorkspace& w = g->ss;
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : g->stream;
+
+  const bool lv_dev = is_device_pointer(levels);
+  const bool par_dev = parents && is_device_pointer(parents);
+  int* d_levels = lv_dev ? levels : nullptr;
+  int* d_parents = par_dev ? parents : nullptr;
+  if (!lv_dev) {
+    if ((st = w.levels_tmp.ensure((size_t)g->V * 4))) return st;
+    d_levels = w.levels_tmp.as<int>();
+  }
+  if (parents && !par_dev) {
+    if ((st = w.parents_tmp.ensure((size_t)g->V * 4))) return st;
+    d_parents = w.parents_tmp.as<int>();
+  }
+  if (o.policy == XBFS_POLICY_FORCED) {
+    if (o.n_forced > w.forced_cap) {
+      if ((st = w.forced.ensure((size_t)o.n_forced))) return st;
+      w.forced_cap = o.n_forced;
+    }
+    XBFS_CUDA_TRY(cudaMemcpyAsync(w.forced.p, o.forced, (size_t)o.n_forced, cudaMemcpyHostToDevice, s));
+  }
+
+  Params p;
+  memset(&p, 0, sizeof(p));
+  p.beg = g->beg.as<long long>();
+  p.csr = g->csr.as<int>();
+  p.V = g->V;
+  p.E = g->E;
+  p.levels = d_levels;
+  p.parents = d_parents;
+  uint32_t* bits = w.bits.as<uint32_t>();
+  p.vis = bits;
+  for (int i = 0; i < 4; ++i) p.fb[i] = bits + (size_t)(i + 1) * w.nwords;
+  for (int par = 0; par < 2; ++par)
+    for (int b = 0; b < 3; ++b) {
+      p.qids[par][b] = w.qids[par][b].as<int>();
+      p.qeb[par][b] = w.qeb[par][b].as<unsigned>();
+    }
+  p.ulist = w.ulist.as<int>();
+  p.ctl = w.ctl.as<Ctl>();
+  p.hist = w.hist.as<LevelRecDev>();
+  p.hist_cap = w.hist_cap;
+  p.forced = w.forced.as<signed char>();
+  p.n_forced = o.n_forced;
+  p.nwords = (g->V + 31) / 32;
+  p.n_ni = g->V - g->n_isolated;
+  p.policy = o.policy;
+  p.alpha = o.alpha;
+  p.async_bu = o.async_bu ? 1 : 0;
+  p.small_max = o.small_max;
+  p.medium_max = o.medium_max;
+  p.beamer_alpha = o.beamer_alpha > 0 ? o.beamer_alpha : 14.f;
+  p.beamer_beta = o.beamer_beta > 0 ? o.beamer_beta : 24.f;
+  p.timeout_ns = 10ull * 1000 * 1000 * 1000;
+  p.max_levels = g->V + 2;
+  extern const float* mlp_device_weights(int device);
+  p.mlp = mlp_device_weights(g->device);
+  if (o.policy == XBFS_POLICY_MLP && !p.mlp) p.policy = XBFS_POLICY_HEURISTIC;
+  p.allow_bu = g->symmetric ? 1 : 0;
+
+  const bool par_on = parents != nullptr;
+  const void* kfn = par_on ? (const void*)k_bfs<true> : (const void*)k_bfs<false>;
+  const size_t smem = sizeof(Smem);
+  XBFS_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int nsm = 0, per_sm = 0;
+  XBFS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device));
+  XBFS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kBlock, smem));
+  if (per_sm < 1) return set_error(XBFS_ERR_INTERNAL, "traversal kernel cannot be resident");
+  int grid = nsm * per_sm;
+  if (o.grid_dim > 0 && o.grid_dim < grid) grid = o.grid_dim;
+  w.grid = grid;
+  w.block = kBlock;
+
+  // ---- initial state
+  XBFS_CUDA_TRY(cudaEventRecord(w.ev0, s));
+  XBFS_CUDA_TRY(cudaMemsetAsync(d_levels, 0xff, (size_t)g->V * 4, s));
+  if (par_on) XBFS_CUDA_TRY(cudaMemsetAsync(d_parents, 0xff, (size_t)g->V * 4, s));
+  XBFS_CUDA_TRY(cudaMemcpyAsync(p.vis, g->iso.p, w.nwords * 4, cudaMemcpyDeviceToDevice, s));
+  XBFS_CUDA_TRY(cudaMemsetAsync(p.fb[0], 0, w.nwords * 4 * 4, s));
+  XBFS_CUDA_TRY(cudaMemsetAsync(p.ctl, 0, sizeof(Ctl), s));
+  k_seed<<<1, 32, 0, s>>>(p, src, par_on ? 1 : 0);
+  XBFS_CUDA_TRY(cudaGetLastError());
+  void* args[] = {&p};
+  XBFS_CUDA_TRY(cudaEventRecord(w.evk0, s));
+  XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, smem, s));
+  XBFS_CUDA_TRY(cudaEventRecord(w.ev1, s));
+  Ctl hctl;
+  XBFS_CUDA_TRY(cudaMemcpyAsync(&hctl, p.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+  if (!lv_dev) XBFS_CUDA_TRY(cudaMemcpyAsync(levels, d_levels, (size_t)g->V * 4, cudaMemcpyDeviceToHost, s));
+  if (parents && !par_dev)
+    XBFS_CUDA_TRY(cudaMemcpyAsync(parents, d_parents, (size_t)g->V * 4, cudaMemcpyDeviceToHost, s));
+  XBFS_CUDA_TRY(cudaStreamSynchronize(s));
+  if (hctl.err != 0)
+    return set_error((xbfs_status)hctl.err, "traversal kernel reported %s", xbfs_strerror(hctl.err));
+  w.last_levels = hctl.depth;
+  float ms = 0, kms = 0;
+  XBFS_CUDA_TRY(cudaEventElapsedTime(&ms, w.ev0, w.ev1));
+  XBFS_CUDA_TRY(cudaEventElapsedTime(&kms, w.evk0, w.ev1));
+
+  if (o.trace || stats) {
+    const int nl = std::min(hctl.depth, w.hist_cap);
+    std::vector<LevelRecDev> h(nl);
+    if (nl > 0) XBFS_CUDA_TRY(cudaMemcpy(h.data(), p.hist, sizeof(LevelRecDev) * nl, cudaMemcpyDeviceToHost));
+    w.trace.resize(nl);
+    for (int i = 0; i < nl; ++i) {
+      w.trace[i].level = i;
+      w.trace[i].strategy = h[i].strategy;
+      w.trace[i].n_f = h[i].n_f;
+      w.trace[i].m_f = h[i].m_f;
+      w.trace[i].n_u = h[i].n_u;
+      w.trace[i].m_u = h[i].m_u;
+      w.trace[i].us = (h[i].t1 > h[i].t0) ? (double)(h[i].t1 - h[i].t0) * 1e-3 : 0.0;
+    }
+  }
+  if (stats) {
+    stats->struct_size = (int32_t)sizeof(xbfs_stats);
+    stats->depth = hctl.depth;
+    stats->reached = (int64_t)hctl.reached;
+    stats->edges_mc = (int64_t)(hctl.msum / 2);
+    stats->device_ms = ms;
+    stats->kernel_ms = kms;
+    stats->n_td_queue = hctl.strat_count[0];
+    stats->n_td_scan = hctl.strat_count[1];
+    stats->n_bu = hctl.strat_count[2];
+    stats->n_async = (int32_t)hctl.n_async;
+    stats->total_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  }
+  return XBFS_OK;
+}
+
+}  // namespace xbfs
+
+using namespace xbfs;
+
+extern "C" {
+
+xbfs_status xbfs_bfs(xbfs_graph* gh, int32_t src, int32_t* levels, int32_t* parents, const xbfs_opts* opts,
+                     xbfs_stats* stats) {
+  return bfs_single((Graph*)gh, src, levels, parents, opts, stats);
+}
+
+xbfs_status xbfs_last_trace(xbfs_graph* gh, xbfs_level_trace* out, int32_t cap, int32_t* n) {
+  Graph* g = (Graph*)gh;
+  if (!g || !n) return set_error(XBFS_ERR_INVALID_ARG, "NULL argument");
+  const int total = (int)g->ss.trace.size();
+  *n = total;
+  if (out && cap > 0) memcpy(out, g->ss.trace.data(), sizeof(xbfs_level_trace) * std::min(cap, total));
+  return XBFS_OK;
+}
+
+}  // extern "C"
