@@ -914,7 +914,7 @@ xbfs_status bfs_single(Graph* g, int32_t src, int32_t* levels, int32_t* parents,
   p.forced = w.forced.as<signed char>();
   p.n_forced = o.n_forced;
   p.nwords = (g->V + 31) / 32;
-  p.n_ni = g->V - g->n_isolated;
+  p.n_ni = g->symmetric ? g->V - g->n_isolated : g->V;
   p.policy = o.policy;
   p.alpha = o.alpha;
   p.async_bu = o.async_bu ? 1 : 0;

@@ -224,6 +224,17 @@ xbfs_status graph_finish_upload(Graph* g) {
     XBFS_CUDA_TRY(cudaStreamSynchronize(g->stream));
   }
   g->symmetric = (res.fp_fwd == res.fp_rev);
+  if (!g->symmetric && real_words > 0) {
+    // In a directed CSR an out-degree-0 vertex can still be reached, so only
+    // the padding bits past V may be pre-marked as visited.
+    XBFS_CUDA_TRY(cudaMemsetAsync(g->iso.p, 0, real_words * 4, g->stream));
+    if (g->V % 32) {
+      const uint32_t tail = ~((1u << (g->V % 32)) - 1u);
+      XBFS_CUDA_TRY(cudaMemcpyAsync(g->iso.as<uint32_t>() + real_words - 1, &tail, 4, cudaMemcpyHostToDevice,
+                                    g->stream));
+    }
+    XBFS_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  }
   if (res.bad_csr != ~0ull)
     return set_error(XBFS_ERR_FORMAT, "csr[%llu] is not a vertex id in [0, %lld)",
                      res.bad_csr - 1, (long long)g->V);
