@@ -152,6 +152,18 @@ void xbfs_graph_free(xbfs_graph* g);
 xbfs_status xbfs_bfs(xbfs_graph* g, int32_t src, int32_t* levels, int32_t* parents,
                      const xbfs_opts* opts, xbfs_stats* stats);
 
+/* Batched multi-source BFS: n sources, levels = n x V int32 (source-major,
+ * host or device). Sources are traversed 64 per uint64 word, up to 8 words
+ * (512 sources) per pass. No counterpart in the reference (one source per
+ * process). opts.policy FORCED with forced[0] = XBFS_TD_QUEUE / XBFS_BU pins
+ * the direction; otherwise opts.alpha (default 4 when <= 0.5) sets the
+ * top-down/bottom-up switch on frontier vs unfinished edges. */
+xbfs_status xbfs_bfs_batch(xbfs_graph* g, const int32_t* srcs, int32_t n, int32_t* levels,
+                           const xbfs_opts* opts, xbfs_stats* stats);
+/* Same with an explicit number of uint64 words per vertex (1, 2, 4 or 8). */
+xbfs_status xbfs_bfs_batch_w(xbfs_graph* g, const int32_t* srcs, int32_t n, int32_t* levels,
+                             const xbfs_opts* opts, xbfs_stats* stats, int32_t words_per_vertex);
+
 /* Per-level trace of the last xbfs_bfs call made with opts.trace = 1
  * (replaces the reference's tag[]/ratio[]/iter[] arrays, written to
  * Hybrid_iteration.csv at bfs_gpu_update.cu:270-272). */

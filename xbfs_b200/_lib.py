@@ -127,6 +127,8 @@ SIGNATURES = {
     "xbfs_gen_er_host": (_i32, [_i64, _f64, _u64, _PPI64, _PPI32, _PI64, _PI64]),
     "xbfs_free_host": (None, [_p]),
     "xbfs_pick_sources": (_i32, [_p, _i64, _i32, _u64, _p]),
+    "xbfs_bfs_batch": (_i32, [_p, _p, _i32, _p, C.POINTER(Opts), C.POINTER(Stats)]),
+    "xbfs_bfs_batch_w": (_i32, [_p, _p, _i32, _p, C.POINTER(Opts), C.POINTER(Stats), _i32]),
     "xbfs_mlp_num_params": (_i32, []),
     "xbfs_mlp_set_weights": (_i32, [_i32, _p, _i32]),
     "xbfs_mlp_logits": (_i32, [_i32, _p, _p, _i32, _p]),

@@ -206,6 +206,27 @@ class Graph:
                          strategies={"td_queue": st.n_td_queue, "td_scan": st.n_td_scan, "bu": st.n_bu},
                          n_async=st.n_async, trace=trace)
 
+    def bfs_batch(self, srcs, levels=None, words_per_vertex: int = 0, direction: Optional[str] = None,
+                  alpha: float = 0.0, stream: int = 0) -> BfsResult:
+        """Multi-source BFS: levels[i] is the level array of srcs[i] (n x V int32,
+        numpy or CUDA tensor). ``direction``: None (switch by alpha), "td", "bu"."""
+        srcs = np.ascontiguousarray(srcs, dtype=np.int32)
+        n = len(srcs)
+        if levels is None:
+            levels = np.empty((n, self.V), dtype=np.int32)
+        opts = BfsOptions(alpha=alpha, stream=stream)
+        if direction is not None:
+            opts.policy = "forced"
+            opts.forced = ["bu" if direction == "bu" else "td_queue"]
+        o = opts.to_c()
+        st = Stats()
+        st.struct_size = C.sizeof(Stats)
+        check(lib.xbfs_bfs_batch_w(self._h, srcs.ctypes.data, n, _ptr(levels), C.byref(o), C.byref(st),
+                                   int(words_per_vertex)))
+        return BfsResult(levels=levels, parents=None, depth=st.depth, reached=st.reached, edges_mc=st.edges_mc,
+                         device_ms=st.device_ms, total_ms=st.total_ms, kernel_ms=st.kernel_ms,
+                         strategies={"td_queue": st.n_td_queue, "td_scan": 0, "bu": st.n_bu}, n_async=0)
+
     def last_trace(self) -> list[dict]:
         n = C.c_int32(0)
         check(lib.xbfs_last_trace(self._h, None, 0, C.byref(n)))
