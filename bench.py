@@ -205,7 +205,10 @@ def run_ours(args):
     V, E = g.V, g.E
     beg = g.offsets()
     srcs = pick_sources(beg, args.sources, args.seed + rank)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library launches on it, and the events, the L2
+    # flush and the output tensor all live on it too
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     opts = BfsOptions(policy=args.policy, stream=stream.cuda_stream)
     lv = torch.empty(V, dtype=torch.int32, device="cuda")
     # L2 flush between steps (untimed): write a 256 MB buffer (> 126 MB L2),

@@ -164,10 +164,54 @@ xbfs_status xbfs_bfs_batch(xbfs_graph* g, const int32_t* srcs, int32_t n, int32_
 xbfs_status xbfs_bfs_batch_w(xbfs_graph* g, const int32_t* srcs, int32_t n, int32_t* levels,
                              const xbfs_opts* opts, xbfs_stats* stats, int32_t words_per_vertex);
 
+/* Multi-graph traversal: many graphs (symmetric CSRs on one device) packed
+ * into one arena, one source each, traversed by one persistent launch that is
+ * captured into a CUDA graph and replayed. No counterpart in the reference.
+ * Levels are concatenated: graph i's array starts at level_offsets[i]
+ * (xbfs_multi_info). */
+typedef struct xbfs_multi xbfs_multi;
+xbfs_status xbfs_multi_create(xbfs_graph* const* graphs, int32_t n, int32_t device, xbfs_multi** out);
+xbfs_status xbfs_multi_info(const xbfs_multi* m, int64_t* total_V, int64_t* total_E, int64_t* level_offsets);
+xbfs_status xbfs_multi_bfs(xbfs_multi* m, const int32_t* srcs, int32_t* levels, const xbfs_opts* opts,
+                           xbfs_stats* stats);
+/* Autotuner: times every candidate (threads per CTA 256/512/1024, thread/warp
+ * degree threshold, direction threshold) on these sources and keeps the
+ * fastest for later xbfs_multi_bfs calls. */
+xbfs_status xbfs_multi_tune(xbfs_multi* m, const int32_t* srcs, int32_t reps, int32_t* block,
+                            int32_t* thread_max, float* alpha, float* best_ms);
+xbfs_status xbfs_multi_set_config(xbfs_multi* m, int32_t block, int32_t thread_max, float alpha);
+void xbfs_multi_free(xbfs_multi* m);
+
 /* Per-level trace of the last xbfs_bfs call made with opts.trace = 1
  * (replaces the reference's tag[]/ratio[]/iter[] arrays, written to
  * Hybrid_iteration.csv at bfs_gpu_update.cu:270-272). */
 xbfs_status xbfs_last_trace(xbfs_graph* g, xbfs_level_trace* out, int32_t cap, int32_t* n);
+
+/* Learned direction/strategy switch (no reference counterpart; the
+ * reference's fixed heuristic stays the fallback).
+ * xbfs_level_costs: for every level of a traversal from src, snapshot the
+ * state, run the level once with each strategy (XBFS_TD_QUEUE, XBFS_TD_SCAN,
+ * XBFS_BU) and record its device time in costs[level*3 + strategy] (us);
+ * continue along the cheapest (follow = 0) or the heuristic's choice
+ * (follow = 1). trace[level] gets the level's statistics and the strategy
+ * taken. *n = number of levels. Levels never depend on the strategies. */
+xbfs_status xbfs_level_costs(xbfs_graph* g, int32_t src, int32_t follow, int32_t cap, float* costs,
+                             xbfs_level_trace* trace, int32_t* n);
+/* MLP 8 -> 32 -> 32 -> 3 (ReLU, softmax), packed as [feature mean 8][feature
+ * std 8][W1 32x8][b1 32][W2 32x32][b2 32][W3 3x32][b3 3] = 1,459 floats of
+ * which 1,443 are trained. */
+int32_t xbfs_mlp_num_params(void);
+/* Install weights for XBFS_POLICY_MLP on a device (n = 0 or NULL removes). */
+xbfs_status xbfs_mlp_set_weights(int32_t device, const float* packed, int32_t n);
+/* Forward pass on the device: logits (n x 3) of features (n x 8). */
+xbfs_status xbfs_mlp_logits(int32_t device, const float* packed, const float* feats, int32_t n, float* logits);
+/* Mean softmax cross-entropy loss and its gradient (1,443 floats, trainable
+ * part only) over n labelled samples, computed by the device kernels. */
+xbfs_status xbfs_mlp_grad(int32_t device, const float* packed, const float* feats, const int32_t* labels,
+                          int32_t n, float* grad, float* loss);
+/* Full-batch SGD with momentum on the device; weights updated in place. */
+xbfs_status xbfs_mlp_train(int32_t device, float* packed, const float* feats, const int32_t* labels, int32_t n,
+                           int32_t epochs, float lr, float momentum, float* losses);
 
 /* Synthetic inputs (no reference counterpart: the reference reads datasets
  * converted by CSRGenerator/tuple_text_to_bin.cpp). All generators are

@@ -1,0 +1,70 @@
+"""Learned direction/strategy switch on the GPU: per-level cost collection
+from snapshots, exactness under every policy, and what the trained network
+(shipped as xbfs_b200/switch_mlp.npz) gains over the reference heuristic."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from xbfs_b200 import Graph, gen_grid_host, gen_rmat_host, pick_sources
+
+pytestmark = pytest.mark.gpu
+
+
+def test_level_costs_follow_the_cheapest_strategy_exactly():
+    from xbfs_b200 import learned
+    beg, csr = gen_rmat_host(15, 16, 3)
+    g = Graph.from_csr(beg, csr)
+    for s in pick_sources(beg, 3, 3):
+        ref = oracle.bfs_queue(beg, csr, s)
+        for follow in (0, 1):
+            tr, costs = learned.level_costs(g, int(s), follow=follow)
+            assert len(tr) == ref.max() + 1
+            assert [t["n_f"] for t in tr] == [int((ref == L).sum()) for L in range(len(tr))]
+            assert np.all(costs > 0)
+            sched = [t["strategy_id"] for t in tr]
+            if follow == 0:
+                assert sched == np.argmin(costs, axis=1).tolist()
+            # replaying the schedule that was followed gives the oracle's levels
+            r = g.bfs(int(s), policy="forced", forced=sched)
+            assert np.array_equal(r.levels, ref)
+
+
+def test_random_network_never_changes_levels():
+    from xbfs_b200 import learned
+    rng = np.random.default_rng(0)
+    for seed in range(3):
+        w = learned.init_weights(rng.normal(0, 2, size=(32, 8)).astype(np.float32), seed)
+        learned.install(w)
+        beg, csr = gen_rmat_host(14, 16, 10 + seed)
+        g = Graph.from_csr(beg, csr)
+        for s in pick_sources(beg, 4, seed):
+            r = g.bfs(int(s), policy="mlp", want_parents=True)
+            ref = oracle.bfs_queue(beg, csr, s)
+            assert np.array_equal(r.levels, ref)
+            assert oracle.check_tree(beg, csr, s, r.levels, r.parents) == 0
+    learned.install(None)
+    beg, csr = gen_grid_host(40, 30)
+    g = Graph.from_csr(beg, csr)
+    r = g.bfs(5, policy="mlp")   # no weights installed: falls back to the heuristic
+    assert np.array_equal(r.levels, oracle.bfs_queue(beg, csr, 5))
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(os.path.dirname(__file__)), "xbfs_b200",
+                                                    "switch_mlp.npz")), reason="no trained weights shipped")
+def test_trained_network_gain_over_heuristic():
+    """Held-out R-MAT scale 21 (the training set has no scale-21 ef16 graph):
+    total traversal time over 8 sources with the trained network vs the
+    reference heuristic, identical levels. Prints the gain."""
+    from xbfs_b200 import learned
+    w, meta = learned.load()
+    learned.install(w)
+    res = learned.evaluate([("rmat", 21, 16, 77)], sources=8, seed=5, reps=3, policies=("heuristic", "mlp"))
+    r = res[str(("rmat", 21, 16, 77))]
+    gain = r["heuristic"]["ms"] / r["mlp"]["ms"]
+    print(f"learned switch vs heuristic on R-MAT s21 ef16: {gain:.3f}x "
+          f"({r['heuristic']['ms']:.3f} ms -> {r['mlp']['ms']:.3f} ms, "
+          f"{r['heuristic']['gteps']:.1f} -> {r['mlp']['gteps']:.1f} GTEPS)")
+    assert gain > 1.0
+    learned.install(None)

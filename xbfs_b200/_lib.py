@@ -91,7 +91,7 @@ def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
             f"{LIB_PATH} is missing: build the CUDA library first "
-            "(python -m xbfs_b200.build, or __graft_entry__.build())")
+            "(python xbfs_b200/build.py, or __graft_entry__.build())")
     return C.CDLL(LIB_PATH)
 
 
@@ -129,6 +129,13 @@ SIGNATURES = {
     "xbfs_pick_sources": (_i32, [_p, _i64, _i32, _u64, _p]),
     "xbfs_bfs_batch": (_i32, [_p, _p, _i32, _p, C.POINTER(Opts), C.POINTER(Stats)]),
     "xbfs_bfs_batch_w": (_i32, [_p, _p, _i32, _p, C.POINTER(Opts), C.POINTER(Stats), _i32]),
+    "xbfs_multi_create": (_i32, [C.POINTER(_p), _i32, _i32, C.POINTER(_p)]),
+    "xbfs_multi_info": (_i32, [_p, _PI64, _PI64, _p]),
+    "xbfs_multi_bfs": (_i32, [_p, _p, _p, C.POINTER(Opts), C.POINTER(Stats)]),
+    "xbfs_multi_tune": (_i32, [_p, _p, _i32, _PI32, _PI32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "xbfs_multi_set_config": (_i32, [_p, _i32, _i32, _f32]),
+    "xbfs_multi_free": (None, [_p]),
+    "xbfs_level_costs": (_i32, [_p, _i32, _i32, _i32, _p, C.POINTER(LevelTrace), _PI32]),
     "xbfs_mlp_num_params": (_i32, []),
     "xbfs_mlp_set_weights": (_i32, [_i32, _p, _i32]),
     "xbfs_mlp_logits": (_i32, [_i32, _p, _p, _i32, _p]),

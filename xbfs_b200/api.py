@@ -54,6 +54,7 @@ class BfsOptions:
     beamer_alpha: float = 14.0
     beamer_beta: float = 24.0
     stream: int = 0
+    bu_mode: int = 0   # bottom-up probe shape (xbfs_opts.reserved[0]); 0 = default
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> Opts:
@@ -71,6 +72,7 @@ class BfsOptions:
         o.beamer_alpha = float(self.beamer_alpha)
         o.beamer_beta = float(self.beamer_beta)
         o.stream = self.stream or None
+        o.reserved[0] = int(self.bu_mode)
         if self.forced is not None:
             vals = [STRATEGIES[s] if isinstance(s, str) else int(s) for s in self.forced]
             arr = (C.c_int8 * max(1, len(vals)))(*vals)
@@ -288,3 +290,54 @@ def read_csr(beg_path: str, csr_path: str) -> tuple[np.ndarray, np.ndarray]:
     beg = np.fromfile(beg_path, dtype="<i8")
     csr = np.fromfile(csr_path, dtype="<i4")
     return beg, csr[: int(beg[-1])]
+
+
+class MultiGraph:
+    """Many graphs on one device, one source each, one persistent launch
+    (xbfs_multi_*). Levels come back concatenated; ``split`` cuts them."""
+
+    def __init__(self, graphs: Sequence[Graph], device: int = 0):
+        arr = (C.c_void_p * len(graphs))(*[g.handle.value for g in graphs])
+        h = C.c_void_p()
+        check(lib.xbfs_multi_create(arr, len(graphs), device, C.byref(h)))
+        self._h = h
+        self.graphs = list(graphs)  # keep the handles alive
+        self.n = len(graphs)
+        tv, te = C.c_int64(), C.c_int64()
+        offs = np.empty(self.n, dtype=np.int64)
+        check(lib.xbfs_multi_info(h, C.byref(tv), C.byref(te), offs.ctypes.data))
+        self.total_V, self.total_E, self.offsets = tv.value, te.value, offs
+
+    def bfs(self, srcs, levels=None) -> BfsResult:
+        srcs = np.ascontiguousarray(srcs, dtype=np.int32)
+        if levels is None:
+            levels = np.empty(self.total_V, dtype=np.int32)
+        st = Stats()
+        st.struct_size = C.sizeof(Stats)
+        check(lib.xbfs_multi_bfs(self._h, srcs.ctypes.data, _ptr(levels), None, C.byref(st)))
+        return BfsResult(levels=levels, parents=None, depth=0, reached=0, edges_mc=st.edges_mc,
+                         device_ms=st.device_ms, total_ms=st.total_ms, kernel_ms=st.kernel_ms,
+                         strategies={}, n_async=0)
+
+    def split(self, levels) -> list:
+        return [levels[o:o + g.V] for o, g in zip(self.offsets, self.graphs)]
+
+    def tune(self, srcs, reps: int = 2) -> dict:
+        srcs = np.ascontiguousarray(srcs, dtype=np.int32)
+        b, t, a, ms = C.c_int32(), C.c_int32(), C.c_float(), C.c_float()
+        check(lib.xbfs_multi_tune(self._h, srcs.ctypes.data, reps, C.byref(b), C.byref(t), C.byref(a), C.byref(ms)))
+        return {"block": b.value, "thread_max": t.value, "alpha": a.value, "best_ms": ms.value}
+
+    def set_config(self, block: int, thread_max: int, alpha: float) -> None:
+        check(lib.xbfs_multi_set_config(self._h, block, thread_max, alpha))
+
+    def free(self) -> None:
+        if self._h:
+            lib.xbfs_multi_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -5,7 +5,8 @@ and links ``xbfs_b200/bin/bfs`` (the reference-compatible command line,
 ``csrc/bfs_cli.cpp``) against it. Objects go to ``_build/`` at the repository
 root; a source is recompiled only when it or a header changed.
 
-Usage: ``python -m xbfs_b200.build [-j N] [--force]``.
+Usage: ``python xbfs_b200/build.py [-j N] [--force] [--ptxas-v]`` (run by path: importing
+the package loads the library this script builds).
 """
 from __future__ import annotations
 

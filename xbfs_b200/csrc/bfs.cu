@@ -14,32 +14,41 @@
 //
 // Design (B200-first, not a translation):
 //  * The reference returns to the host every level: it sums frontier edges
-//    with an O(V) host loop, copies the whole status array back, and checks
+//    with an O(V) host loop, copies the whole status array back and checks
 //    termination against the CPU answer. Here the level loop, the statistics
 //    (n_f, m_f, n_u, m_u, reduced inside the kernels) and the strategy
-//    decision live on the device; levels are separated by a bounded grid
-//    barrier (~1-2 us) instead of a host round trip.
+//    decision live on the device; levels are separated by a bounded count-up
+//    grid barrier instead of a host round trip.
 //  * Status is kept twice: the int32 level array (the output contract) and
-//    bitmaps - visited (pre-seeded with isolated vertices), and a ring of four
+//    bitmaps - visited (pre-seeded with isolated vertices) and a ring of four
 //    frontier bitmaps (level L, L+1, L+2 for the asynchronous bottom-up, and
-//    one being cleared). At scale 23 each bitmap is 1 MB, so every random
-//    status probe hits L2 (126 MB), while the CSR is streamed with an
-//    evict-first hint.
-//  * Frontier queues are degree-binned (small / medium / large, thresholds
-//    tunable, reference 32 / 256) and carry an exclusive edge offset per
-//    entry, reserved with one packed 64-bit atomic (count | edges). Expansion
-//    is edge-balanced: each CTA takes an equal slice of each bin's edge space
-//    and walks its owners with a shared-memory window, so a hub vertex with
-//    10^5 neighbours is spread over the whole GPU instead of one CTA.
-//  * Winners are staged per CTA in shared memory and flushed with one global
-//    atomic per bin per flush instead of one atomicAdd per vertex.
-//  * Bottom-up builds a ballot/popcount-compacted, sorted list of unvisited
-//    vertices per CTA (the reference's ballot_counting + prefix sum + FQ_gen,
-//    without the host round trip of my_prefixsum), then warps drain it with
-//    early exit and the reference's asynchronous level+2 rule.
+//    one being cleared). At scale 23 a bitmap is 1 MB, so random status
+//    probes hit L2 (126 MB) while the CSR streams with an evict-first hint.
+//  * Frontier queues are degree-binned (small / medium / large, reference
+//    thresholds 32 / 256). Every entry carries the vertex, its CSR offset and
+//    an exclusive edge offset, reserved with one packed 64-bit atomic
+//    (edges | count). Every bin is expanded edge-balanced: each CTA takes an
+//    equal slice of the bin's edge space and walks its owners through a
+//    shared-memory window, so a hub with 10^5 neighbours is spread over the
+//    whole GPU and a lone degree-18 source costs one round, not 18 steps of one
+//    thread (the reference maps bins to thread / warp / CTA per vertex; the
+//    bins survive here as the processing order and the queue split).
+//  * Top-down winners are staged per CTA in shared memory and flushed with
+//    one global atomic per bin per flush.
+//  * A top-down level whose frontier is only in bitmap form (after bottom-up
+//    or single-scan) compacts and expands the bitmap in the same phase
+//    ("single scan"), CTA by CTA, instead of building a queue first.
+//  * Bottom-up: every warp takes 1024-vertex chunks from a global counter,
+//    compacts the chunk's unvisited vertices with a warp popcount scan (the
+//    reference's ballot_counting + prefix sum + FQ_gen, without the host round
+//    trip of my_prefixsum) and lanes probe eight neighbours at a time with
+//    early exit and the reference's asynchronous level+2 rule; no CTA-wide
+//    synchronisation until the level ends.
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
+
+#include <limits.h>
 
 #include <algorithm>
 #include <chrono>
@@ -52,10 +61,14 @@ namespace xbfs {
 constexpr int kBlock = 512;         // threads per CTA of the traversal kernel
 constexpr int kK = 2;               // edges per thread per gather round
 constexpr int kTE = kBlock * kK;    // edges per gather round
+constexpr int kWin = 2048;          // shared window / tile list capacity
 constexpr int kCap = 2048;          // staging capacity, small and medium bins
-constexpr int kCapL = 512;          // staging capacity, large bin
+constexpr int kCapL = 256;          // staging capacity, large bin
 constexpr int kFlushAt = kCap - kTE;
 constexpr int kFlushAtL = kCapL / 2;  // large-bin overflow goes straight to the global queue
+constexpr int kTileW = kWin / 32;   // bitmap words per dense fused-sweep sub-tile
+constexpr int kBuChunkW = 32;       // bitmap words per bottom-up warp chunk (1024 vertices)
+constexpr int kHeavyDeg = 4096;     // fused sweep: larger degrees are deferred to the heavy list
 
 constexpr unsigned long long kCountMask = (1ull << 31) - 1;
 
@@ -82,11 +95,17 @@ struct Ctl {
   unsigned long long n_async;   // vertices given level+2 by bottom-up
   unsigned long long reached;   // sum of frontier sizes
   unsigned long long msum;      // sum of frontier degrees
+  unsigned long long heavy[2];  // packed counter of the heavy list, by level parity
+  unsigned int bu_chunk[2];     // bottom-up chunk dispenser, by level parity
   int strat_count[4];
   FDesc fd[4];
 };
 
-struct MlpWeights;  // mlp.cu
+struct QBin {
+  int* ids;
+  unsigned* eb;    // exclusive edge offset within the bin
+  long long* bg;   // CSR offset of the vertex
+};
 
 struct Params {
   const long long* beg;
@@ -96,9 +115,8 @@ struct Params {
   int* parents;
   uint32_t* vis;
   uint32_t* fb[4];
-  int* qids[2][3];
-  unsigned* qeb[2][3];
-  int* ulist;
+  QBin q[2][3];
+  QBin heavy;
   Ctl* ctl;
   LevelRecDev* hist;
   int hist_cap;
@@ -115,29 +133,37 @@ struct Params {
   long long max_levels;
   const float* mlp;  // packed MLP weights (may be null)
   int allow_bu;      // 0 when the CSR is not symmetric: bottom-up would miss parents
+  struct ResumeState* rs;  // stepped mode: state saved at stop_level / loaded when resume
+  long long stop_level;
+  int resume;
+  int bu_mode;       // bottom-up neighbour probe shape (see probe_range)
 };
 
 // ---------------------------------------------------------------------------
 // Shared memory layout of the traversal kernel (dynamic).
 // ---------------------------------------------------------------------------
 struct __align__(16) Smem {
-  long long wbeg[kTE + 1];
-  unsigned web[kTE + 1];
-  int wu[kTE + 1];
+  long long wbeg[kWin + 1];   // window / tile: CSR offsets
+  unsigned web[kWin + 1];     // window / tile: edge offsets
+  int wu[kWin + 1];           // window / tile: vertices (also the bottom-up list)
   int st_id[2][kCap];
   int st_deg[2][kCap];
+  long long st_bg[2][kCap];
   int stl_id[kCapL];
   int stl_deg[kCapL];
+  long long stl_bg[kCapL];
   int cnt[3];
   int strategy;
   int next_s;
   int bu_next;
   int bu_n;
-  int flag;
+  int chunk;
+  unsigned long long bins[3];   // F_L bin counters, read once per level
+  long long pend_next;          // F_{L+1} entries already found (async bottom-up)
   unsigned long long base_slot, base_edge;
   long long red[kBlock / 32 + 1];
+  long long red4[4 * (kBlock / 32)];
   float mlp_h[2][32];
-  int go;
 };
 
 __device__ __forceinline__ int bin_of(long long d, int small_max, int medium_max) {
@@ -160,6 +186,16 @@ struct PolicyState {
   // features
   long long n_prev;
   int prev_strategy;
+};
+
+// Loop state carried across launches in stepped mode (xbfs_level_costs): a
+// launch stops at the top of level `stop_level` and the next one resumes there.
+struct ResumeState {
+  long long L;
+  int q_valid, b_valid;
+  unsigned dirty;
+  long long vis_n, vis_m;
+  PolicyState ps;
 };
 
 constexpr long long kInfinite = 10000;  // bfs_adaptiveFQ_wb_async.cuh:29
@@ -260,32 +296,35 @@ __device__ __forceinline__ float flog(double x) { return (float)log1p(x > 0 ? x 
 // Staging of top-down winners (per CTA) and flush to the global binned queue.
 // ---------------------------------------------------------------------------
 struct QOut {
-  int* ids[3];
-  unsigned* eb[3];
+  QBin b[3];
   unsigned long long* ctr;  // fd[..].bin
 };
 
-__device__ __forceinline__ void direct_enqueue(const QOut& q, int bin, int v, long long d) {
-  unsigned long long old = atomicAdd(&q.ctr[bin], ((unsigned long long)d << 31) | 1ull);
-  unsigned long long slot = old & kCountMask;
-  q.ids[bin][slot] = v;
-  q.eb[bin][slot] = (unsigned)(old >> 31);
+__device__ __forceinline__ void direct_enqueue(const QBin& q, unsigned long long* ctr, int v, long long d,
+                                               long long bg) {
+  const unsigned long long old = atomicAdd(ctr, ((unsigned long long)d << 31) | 1ull);
+  const unsigned long long slot = old & kCountMask;
+  q.ids[slot] = v;
+  q.eb[slot] = (unsigned)(old >> 31);
+  q.bg[slot] = bg;
 }
 
-__device__ __forceinline__ void stage(Smem& sm, const QOut& q, int bin, int v, long long d) {
-  int slot = atomicAdd(&sm.cnt[bin], 1);
+__device__ __forceinline__ void stage(Smem& sm, const QOut& q, int bin, int v, long long d, long long bg) {
+  const int slot = atomicAdd(&sm.cnt[bin], 1);
   if (bin < 2) {
     if (slot < kCap) {
       sm.st_id[bin][slot] = v;
       sm.st_deg[bin][slot] = (int)d;
+      sm.st_bg[bin][slot] = bg;
       return;
     }
   } else if (slot < kCapL) {
     sm.stl_id[slot] = v;
     sm.stl_deg[slot] = (int)d;
+    sm.stl_bg[slot] = bg;
     return;
   }
-  direct_enqueue(q, bin, v, d);
+  direct_enqueue(q.b[bin], &q.ctr[bin], v, d, bg);
 }
 
 // Block-wide flush of all staged winners (call from all threads, uniform).
@@ -296,29 +335,33 @@ __device__ void flush(Smem& sm, const QOut& q) {
     int n = sm.cnt[bin];
     if (n > cap) n = cap;
     if (n == 0) continue;
-    int* ids = bin < 2 ? sm.st_id[bin] : sm.stl_id;
-    int* degs = bin < 2 ? sm.st_deg[bin] : sm.stl_deg;
-    // each thread owns a contiguous run of PER items
+    const int* ids = bin < 2 ? sm.st_id[bin] : sm.stl_id;
+    const int* degs = bin < 2 ? sm.st_deg[bin] : sm.stl_deg;
+    const long long* bgs = bin < 2 ? sm.st_bg[bin] : sm.stl_bg;
     constexpr int PER = (kCap + kBlock - 1) / kBlock;
     const int i0 = threadIdx.x * PER;
     long long loc = 0;
+#pragma unroll
     for (int k = 0; k < PER; ++k)
       if (i0 + k < n) loc += degs[i0 + k];
     long long total;
-    long long ex = block_exclusive_scan<kBlock, long long>(loc, sm.red, &total);
+    const long long ex = block_exclusive_scan<kBlock, long long>(loc, sm.red, &total);
     if (threadIdx.x == 0) {
-      unsigned long long old = atomicAdd(&q.ctr[bin], ((unsigned long long)total << 31) | (unsigned long long)n);
+      const unsigned long long old =
+          atomicAdd(&q.ctr[bin], ((unsigned long long)total << 31) | (unsigned long long)n);
       sm.base_slot = old & kCountMask;
       sm.base_edge = old >> 31;
     }
     __syncthreads();
     const unsigned long long bs = sm.base_slot, be = sm.base_edge;
     long long run = ex;
+#pragma unroll
     for (int k = 0; k < PER; ++k) {
-      int i = i0 + k;
+      const int i = i0 + k;
       if (i < n) {
-        q.ids[bin][bs + i] = ids[i];
-        q.eb[bin][bs + i] = (unsigned)(be + run);
+        q.b[bin].ids[bs + i] = ids[i];
+        q.b[bin].eb[bs + i] = (unsigned)(be + run);
+        q.b[bin].bg[bs + i] = bgs[i];
         run += degs[i];
       }
     }
@@ -340,6 +383,7 @@ struct Acc {
   long long n2, m2;  // level+2 (asynchronous bottom-up)
 };
 
+// Top-down claim of v (reached from u) for level L+1.
 template <bool PAR>
 __device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& q, Acc& acc, int v, int u,
                                          int L, bool enq, uint32_t* fbn) {
@@ -349,18 +393,19 @@ __device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& 
   if (old & bit) return;
   p.levels[v] = L + 1;
   if (PAR) p.parents[v] = u;
-  const long long d = ld_nc_i64(p.beg + v + 1) - ld_nc_i64(p.beg + v);
+  const long long b0 = ld_nc_i64(p.beg + v);
+  const long long d = ld_nc_i64(p.beg + v + 1) - b0;
   acc.n1 += 1;
   acc.m1 += d;
   if (enq) {
-    if (d > 0) stage(sm, q, bin_of(d, p.small_max, p.medium_max), v, d);
+    if (d > 0) stage(sm, q, bin_of(d, p.small_max, p.medium_max), v, d, b0);
   } else {
     red_or_u32(fbn + word, bit);
   }
 }
 
-// Warp 0 finds the last slot s in [0, cnt) with eb[s] <= key (eb strictly
-// increasing, eb[0] == 0 <= key). 32-ary search.
+// Warp-parallel search: last slot s in [0, cnt) with eb[s] <= key (eb strictly
+// increasing from eb[0] = 0 <= key). Called by a full warp.
 __device__ int find_owner(const unsigned* eb, unsigned cnt, unsigned long long key) {
   const int lane = threadIdx.x & 31;
   unsigned lo = 0, hi = cnt;  // answer in [lo, hi)
@@ -381,17 +426,27 @@ __device__ int find_owner(const unsigned* eb, unsigned cnt, unsigned long long k
   return (int)(lo + 31 - __clz(mask));
 }
 
-// Edge-balanced expansion of one bin of the current frontier queue.
+// last index a in [0, n) with web[a] <= e (web non-decreasing, web[0] <= e)
+__device__ __forceinline__ int smem_owner(const unsigned* web, int n, unsigned long long e) {
+  int a = 0, c = n;
+  while (c - a > 1) {
+    const int mid = (a + c) >> 1;
+    if ((unsigned long long)web[mid] <= e) a = mid; else c = mid;
+  }
+  return a;
+}
+
+// Edge-balanced expansion of one bin of the current frontier queue (medium
+// and large bins, and the heavy list of a fused sweep).
 template <bool PAR>
-__device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, const int* ids,
-                           const unsigned* eb, unsigned cnt, unsigned long long M, int L, bool enq,
-                           uint32_t* fbn) {
+__device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
+                           unsigned long long M, int L, bool enq, uint32_t* fbn) {
   if (cnt == 0 || M == 0) return;
   const unsigned long long G = gridDim.x, b = blockIdx.x;
   const unsigned long long lo = M * b / G, hi = M * (b + 1) / G;
   if (lo >= hi) return;
   if (threadIdx.x < 32) {
-    int s = find_owner(eb, cnt, lo);
+    const int s = find_owner(in.eb, cnt, lo);
     if (threadIdx.x == 0) sm.next_s = s;
   }
   __syncthreads();
@@ -402,12 +457,11 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
       const unsigned slot = s + (unsigned)i;
       unsigned e0 = 0xffffffffu;
       if (slot < cnt) {
-        const unsigned x = eb[slot];
+        const unsigned x = in.eb[slot];
         if ((unsigned long long)x < rhi) {
           e0 = x;
-          const int u = ids[slot];
-          sm.wu[i] = u;
-          sm.wbeg[i] = ld_nc_i64(p.beg + u);
+          sm.wu[i] = in.ids[slot];
+          sm.wbeg[i] = in.bg[slot];
         }
       }
       sm.web[i] = e0;
@@ -417,55 +471,112 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
     for (int k = 0; k < kK; ++k) {
       const unsigned long long e = r + threadIdx.x + (unsigned long long)k * kBlock;
       if (e < rhi) {
-        // owner: last i with web[i] <= e
-        int a = 0, c = kTE + 1;
-        while (c - a > 1) {
-          const int mid = (a + c) >> 1;
-          if ((unsigned long long)sm.web[mid] <= e) a = mid; else c = mid;
-        }
-        const int u = sm.wu[a];
-        const long long idx = sm.wbeg[a] + (long long)(e - sm.web[a]);
-        const int v = ld_stream_i32(p.csr + idx);
-        claim_td<PAR>(p, sm, q, acc, v, u, L, enq, fbn);
+        const int a = smem_owner(sm.web, kTE + 1, e);
+        const int v = ld_stream_i32(p.csr + sm.wbeg[a] + (long long)(e - sm.web[a]));
+        claim_td<PAR>(p, sm, q, acc, v, sm.wu[a], L, enq, fbn);
       }
     }
-    if (threadIdx.x == 0 && rhi < hi) {
-      int a = 0, c = kTE + 1;
-      while (c - a > 1) {
-        const int mid = (a + c) >> 1;
-        if ((unsigned long long)sm.web[mid] <= rhi) a = mid; else c = mid;
-      }
-      sm.next_s = (int)(s + a);
-    }
+    if (threadIdx.x == 0 && rhi < hi) sm.next_s = (int)(s + smem_owner(sm.web, kTE + 1, rhi));
     __syncthreads();
     s = (unsigned)sm.next_s;
     if (enq && need_flush(sm)) flush(sm, q);
   }
 }
 
-// Bitmap of frontier L -> binned queue of frontier L (degree-0 vertices are
-// never queued, as in the reference's bins). Ballot-free: each thread owns one
-// word and emits its set bits one per sub-round so a sub-round stages at most
-// kBlock entries.
-__device__ void sweep_bitmap_to_queue(const Params& p, Smem& sm, const QOut& q, const uint32_t* fbc) {
+// Top-down from a frontier held only as a bitmap ("single scan"): every CTA
+// compacts the set bits of its slice tile by tile into shared memory, gives
+// each vertex of degree <= kHeavyDeg its exclusive edge offset with a block
+// scan and expands the tile edge-balanced; heavier vertices go to a global
+// list expanded grid-wide after the barrier.
+template <bool PAR>
+__device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc, const uint32_t* fbc, int L,
+                              bool enq, uint32_t* fbn, int par) {
   const long long nw = p.nwords;
-  const long long ntile = (nw + kBlock - 1) / kBlock;
-  for (long long t = blockIdx.x; t < ntile; t += gridDim.x) {
-    const long long w = t * kBlock + threadIdx.x;
-    uint32_t bits = (w < nw) ? ld_cg_u32(fbc + w) : 0u;
-    while (__syncthreads_or(bits != 0)) {
-      if (bits) {
-        const int bpos = __ffs(bits) - 1;
+  const long long G = gridDim.x, b = blockIdx.x;
+  const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
+  unsigned long long* hctr = &p.ctl->heavy[par];
+  // A tile is kBlock words (one per thread) when its set bits fit the shared
+  // window (the common, sparse case); a denser tile is cut into sub-tiles of
+  // kTileW words, which always fit.
+  for (long long wt = w0; wt < w1; wt += kBlock) {
+    uint32_t tbits = 0;
+    {
+      const long long w = wt + threadIdx.x;
+      if (w < w1) tbits = ld_cg_u32(fbc + w);
+    }
+    const int tcount = __syncthreads_count(tbits != 0);
+    if (tcount == 0) continue;
+    long long tsum = block_sum<kBlock, long long>((long long)__popc(tbits), sm.red);
+    const bool whole = tsum <= kWin;
+    const long long wend = (wt + kBlock < w1) ? wt + kBlock : w1;
+  for (long long wb = wt; wb < wend; wb += whole ? kBlock : kTileW) {
+    // 1. compact the set bits of the (sub-)tile
+    uint32_t bits = 0;
+    const long long w = wb + threadIdx.x;
+    if (whole) bits = tbits;
+    else if (threadIdx.x < kTileW && w < wend) bits = ld_cg_u32(fbc + w);
+    long long total;
+    const long long ex = block_exclusive_scan<kBlock, long long>((long long)__popc(bits), sm.red, &total);
+    {
+      int o = (int)ex;
+      while (bits) {
+        const int bp = __ffs(bits) - 1;
         bits &= bits - 1;
-        const int v = (int)(w * 32 + bpos);
-        const long long d = ld_nc_i64(p.beg + v + 1) - ld_nc_i64(p.beg + v);
-        if (d > 0) stage(sm, q, bin_of(d, p.small_max, p.medium_max), v, d);
+        sm.wu[o++] = (int)(w * 32 + bp);
+      }
+    }
+    __syncthreads();
+    const int n = (int)total;
+    if (n == 0) continue;
+    // 2. degrees and CSR offsets; heavy vertices are deferred
+    constexpr int PER = (kWin + kBlock - 1) / kBlock;
+    const int i0 = threadIdx.x * PER;
+    long long loc = 0;
+    int dd[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      dd[k] = 0;
+      const int i = i0 + k;
+      if (i < n) {
+        const int u = sm.wu[i];
+        const long long b0 = ld_nc_i64(p.beg + u);
+        const long long d = ld_nc_i64(p.beg + u + 1) - b0;
+        sm.wbeg[i] = b0;
+        if (d > kHeavyDeg) {
+          direct_enqueue(p.heavy, hctr, u, d, b0);
+        } else {
+          dd[k] = (int)d;
+          loc += d;
+        }
+      }
+    }
+    long long T;
+    long long run = block_exclusive_scan<kBlock, long long>(loc, sm.red, &T);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int i = i0 + k;
+      if (i < n) {
+        sm.web[i] = (unsigned)run;
+        run += dd[k];
+      }
+    }
+    __syncthreads();
+    // 3. edge-balanced expansion of the tile
+    for (long long r = 0; r < T; r += kTE) {
+#pragma unroll
+      for (int k = 0; k < kK; ++k) {
+        const long long e = r + threadIdx.x + (long long)k * kBlock;
+        if (e < T) {
+          const int a = smem_owner(sm.web, n, (unsigned long long)e);
+          const int v = __ldg(p.csr + sm.wbeg[a] + (e - (long long)sm.web[a]));
+          claim_td<PAR>(p, sm, q, acc, v, sm.wu[a], L, enq, fbn);
+        }
       }
       __syncthreads();
-      if (need_flush(sm)) flush(sm, q);
+      if (enq && need_flush(sm)) flush(sm, q);
     }
   }
-  flush(sm, q);
+  }
 }
 
 // Queue of frontier L -> bitmap of frontier L.
@@ -474,7 +585,7 @@ __device__ void scatter_queue_to_bitmap(const Params& p, int par, const FDesc& f
   const long long nth = (long long)gridDim.x * kBlock;
   for (int bin = 0; bin < 3; ++bin) {
     const long long cnt = (long long)(ld_cg_u64(&fd.bin[bin]) & kCountMask);
-    const int* ids = p.qids[par][bin];
+    const int* ids = p.q[par][bin].ids;
     for (long long i = tid; i < cnt; i += nth) {
       const int v = ids[i];
       red_or_u32(fbc + (v >> 5), 1u << (v & 31));
@@ -482,93 +593,126 @@ __device__ void scatter_queue_to_bitmap(const Params& p, int par, const FDesc& f
   }
 }
 
-// Bottom-up step for level L over this CTA's slice of the vertex range.
+// Bottom-up neighbour probe: scans [e, e_end) PW neighbours at a time (their
+// CSR entries and frontier bits loaded together) until a level-L parent is
+// found; with ASYNC, remembers the first level-(L+1) neighbour on the way.
+template <int PW, bool LDG, bool ASYNC>
+__device__ __forceinline__ void probe_range(const Params& p, const uint32_t* fbc, const uint32_t* fbn,
+                                            long long& e, long long e_end, int& found, int& found2) {
+  for (; e < e_end; e += PW) {
+    int u[PW];
+#pragma unroll
+    for (int k = 0; k < PW; ++k)
+      u[k] = (e + k < e_end) ? (LDG ? __ldg(p.csr + e + k) : ld_stream_i32(p.csr + e + k)) : -1;
+    uint32_t wc[PW];
+#pragma unroll
+    for (int k = 0; k < PW; ++k) wc[k] = (u[k] >= 0) ? fbc[u[k] >> 5] : 0u;
+#pragma unroll
+    for (int k = 0; k < PW; ++k)
+      if (found < 0 && u[k] >= 0 && ((wc[k] >> (u[k] & 31)) & 1u)) found = u[k];
+    if (found >= 0) return;
+    if (ASYNC && found2 < 0) {
+      uint32_t wn[PW];
+#pragma unroll
+      for (int k = 0; k < PW; ++k) wn[k] = (u[k] >= 0) ? ld_cg_u32(fbn + (u[k] >> 5)) : 0u;
+#pragma unroll
+      for (int k = 0; k < PW; ++k)
+        if (found2 < 0 && u[k] >= 0 && ((wn[k] >> (u[k] & 31)) & 1u)) found2 = u[k];
+    }
+  }
+}
+
+// Bottom-up step for level L. CTAs take 2048-vertex chunks from a global
+// dispenser, compact the unvisited vertices of a chunk (sorted) into shared
+// memory and let each lane search one vertex's neighbours, eight at a time.
 template <bool PAR, bool ASYNC>
 __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
                           uint32_t* fbn2) {
   const long long nw = p.nwords;
-  const long long G = gridDim.x, b = blockIdx.x;
-  const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
-  int* list = p.ulist + w0 * 32;
-  // 1. ballot/popcount compaction of unvisited vertices into a sorted list
-  long long pos = 0;
-  for (long long wb = w0; wb < w1; wb += kBlock) {
-    const long long w = wb + threadIdx.x;
-    uint32_t bits = (w < w1) ? ~ld_cg_u32(p.vis + w) : 0u;
-    long long total;
-    const long long ex = block_exclusive_scan<kBlock, long long>((long long)__popc(bits), sm.red, &total);
-    long long o = pos + ex;
-    while (bits) {
-      const int bp = __ffs(bits) - 1;
-      bits &= bits - 1;
-      list[o++] = (int)(w * 32 + bp);
-    }
-    pos += total;
-  }
-  if (threadIdx.x == 0) {
-    sm.bu_next = 0;
-    sm.bu_n = (int)pos;
-  }
-  __syncthreads();
-  const int n = sm.bu_n;
+  const long long nchunks = (nw + kBuChunkW - 1) / kBuChunkW;
+  unsigned* disp = &p.ctl->bu_chunk[L & 1];
   const int lane = threadIdx.x & 31;
-  // 2. warps drain the list 32 entries at a time
+  // Each warp works alone: it takes a 1024-vertex chunk from the dispenser,
+  // compacts the chunk's unvisited vertices (lane = bitmap word, warp scan of
+  // the popcounts) into its own shared list, and drains it 32 at a time. The
+  // lists alias the top-down staging area, which is idle during bottom-up.
+  static_assert(sizeof(int) * 2 * kCap * 2 + sizeof(long long) * 2 * kCap >=
+                    sizeof(int) * (kBlock / 32) * kBuChunkW * 32,
+                "bottom-up lists must fit in the staging area");
+  int* list = reinterpret_cast<int*>(&sm.st_id[0][0]) + (threadIdx.x >> 5) * (kBuChunkW * 32);
   for (;;) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(&sm.bu_next, 32);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    const int i = base + lane;
-    if (i < n) {
-      const int v = list[i];
-      const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
-      int found = -1, found2 = -1;
-      for (long long e = e0; e < e1; e += 4) {
-        int u[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) u[k] = (e + k < e1) ? ld_stream_i32(p.csr + e + k) : -1;
-        uint32_t wc[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) wc[k] = (u[k] >= 0) ? fbc[u[k] >> 5] : 0u;
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-          if (found < 0 && u[k] >= 0 && ((wc[k] >> (u[k] & 31)) & 1u)) found = u[k];
-        if (found >= 0) break;
-        if (ASYNC && found2 < 0) {
-#pragma unroll
-          for (int k = 0; k < 4; ++k)
-            if (found2 < 0 && u[k] >= 0 && ((ld_cg_u32(fbn + (u[k] >> 5)) >> (u[k] & 31)) & 1u)) found2 = u[k];
+    unsigned c = 0;
+    if (lane == 0) c = atomicAdd(disp, 1u);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if ((long long)c >= nchunks) break;
+    const long long w = (long long)c * kBuChunkW + lane;
+    uint32_t bits = (w < nw) ? ~ld_cg_u32(p.vis + w) : 0u;
+    const int cb = __popc(bits);
+    const int incl = warp_inclusive_scan(cb);
+    const int n = __shfl_sync(0xffffffffu, incl, 31);
+    {
+      int o = incl - cb;
+      while (bits) {
+        const int bp = __ffs(bits) - 1;
+        bits &= bits - 1;
+        list[o++] = (int)(w * 32 + bp);
+      }
+    }
+    __syncwarp();
+    for (int base = 0; base < n; base += 32) {
+      const int i = base + lane;
+      if (i < n) {
+        const int v = list[i];
+        const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
+        int found = -1, found2 = -1;
+        long long e = e0;
+        switch (p.bu_mode) {
+          case 1:  // 4 at a time, streaming loads
+            probe_range<4, false, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+            break;
+          case 2:  // 8 at a time, L1-allocating loads
+            probe_range<8, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+            break;
+          case 3:  // 4 at a time, L1-allocating loads
+            probe_range<4, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+            break;
+          case 4:  // widening 2 / 4 / 8, L1-allocating loads
+            probe_range<2, true, ASYNC>(p, fbc, fbn, e, e0 + 2 < e1 ? e0 + 2 : e1, found, found2);
+            if (found < 0) probe_range<4, true, ASYNC>(p, fbc, fbn, e, e0 + 6 < e1 ? e0 + 6 : e1, found, found2);
+            if (found < 0) probe_range<8, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+            break;
+          default:  // widening 2 / 4 / 8, streaming loads
+            probe_range<2, false, ASYNC>(p, fbc, fbn, e, e0 + 2 < e1 ? e0 + 2 : e1, found, found2);
+            if (found < 0) probe_range<4, false, ASYNC>(p, fbc, fbn, e, e0 + 6 < e1 ? e0 + 6 : e1, found, found2);
+            if (found < 0) probe_range<8, false, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+        }
+        const uint32_t word = (uint32_t)v >> 5, bit = 1u << (v & 31);
+        if (found >= 0) {
+          p.levels[v] = L + 1;
+          if (PAR) p.parents[v] = found;
+          red_or_u32(p.vis + word, bit);
+          red_or_u32(fbn + word, bit);
+          acc.n1 += 1;
+          acc.m1 += e1 - e0;
+        } else if (ASYNC && found2 >= 0) {
+          p.levels[v] = L + 2;
+          if (PAR) p.parents[v] = found2;
+          red_or_u32(p.vis + word, bit);
+          red_or_u32(fbn2 + word, bit);
+          acc.n2 += 1;
+          acc.m2 += e1 - e0;
         }
       }
-      const uint32_t word = (uint32_t)v >> 5, bit = 1u << (v & 31);
-      if (found >= 0) {
-        p.levels[v] = L + 1;
-        if (PAR) p.parents[v] = found;
-        red_or_u32(p.vis + word, bit);
-        red_or_u32(fbn + word, bit);
-        acc.n1 += 1;
-        acc.m1 += e1 - e0;
-      } else if (ASYNC && found2 >= 0) {
-        p.levels[v] = L + 2;
-        if (PAR) p.parents[v] = found2;
-        red_or_u32(p.vis + word, bit);
-        red_or_u32(fbn2 + word, bit);
-        acc.n2 += 1;
-        acc.m2 += e1 - e0;
-      }
     }
+    __syncwarp();
   }
 }
 
 // Block-reduce the accumulators and publish them to the frontier descriptors.
 __device__ void publish_acc(Smem& sm, Acc& acc, FDesc* f1, FDesc* f2) {
-  long long n1 = block_sum<kBlock, long long>(acc.n1, sm.red);
-  long long m1 = block_sum<kBlock, long long>(acc.m1, sm.red);
-  long long n2 = 0, m2 = 0;
-  if (f2) {
-    n2 = block_sum<kBlock, long long>(acc.n2, sm.red);
-    m2 = block_sum<kBlock, long long>(acc.m2, sm.red);
-  }
+  long long v[4] = {acc.n1, acc.m1, acc.n2, acc.m2};
+  block_sum_n<kBlock, 4, long long>(v, sm.red4);
+  const long long n1 = v[0], m1 = v[1], n2 = v[2], m2 = v[3];
   if (threadIdx.x == 0) {
     if (n1) atomicAdd(&f1->n, (unsigned long long)n1);
     if (m1) atomicAdd(&f1->m, (unsigned long long)m1);
@@ -610,14 +754,42 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
   ps.bu_dir = 0;
   ps.n_prev = 1;
   ps.prev_strategy = XBFS_TD_QUEUE;
-  long long vis_n = 0, vis_m = 0;  // sum over frontiers <= L (thread 0)
+  long long vis_n = 0, vis_m = 0;  // sums over frontiers <= L (thread 0)
+  // statistics of the whole traversal, kept by thread 0 of block 0
+  unsigned long long st_reached = 0, st_msum = 0, st_async = 0;
+  int st_strat[3] = {0, 0, 0};
 
   bool q_valid = true, b_valid = true;
   unsigned dirty = 1u;  // fb[i] may contain set bits
   Acc acc{0, 0, 0, 0};
   const uint32_t nb = gridDim.x;
+  uint32_t epoch = 0;
   long long L = 0;
+  if (p.resume) {
+    const ResumeState r = *p.rs;
+    L = r.L;
+    q_valid = r.q_valid != 0;
+    b_valid = r.b_valid != 0;
+    dirty = r.dirty;
+    vis_n = r.vis_n;
+    vis_m = r.vis_m;
+    ps = r.ps;
+  }
   for (;; ++L) {
+    if (L >= p.stop_level) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ResumeState r;
+        r.L = L;
+        r.q_valid = q_valid;
+        r.b_valid = b_valid;
+        r.dirty = dirty;
+        r.vis_n = vis_n;
+        r.vis_m = vis_m;
+        r.ps = ps;
+        *p.rs = r;
+      }
+      break;
+    }
     if (L >= p.max_levels) {
       if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctl->err, 0, (int)XBFS_ERR_INTERNAL);
       break;
@@ -627,21 +799,31 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
     FDesc* F2 = &ctl->fd[(L + 2) & 3];
     FDesc* F3 = &ctl->fd[(L + 3) & 3];
     if (threadIdx.x == 0) {
+      // every descriptor word this level needs, loaded together
       const long long n_f = (long long)ld_cg_u64(&F0->n);
       const long long m_f = (long long)ld_cg_u64(&F0->m);
+      const long long pn = (long long)ld_cg_u64(&F1->pend_n);
+      const long long pm = (long long)ld_cg_u64(&F1->pend_m);
+      const long long own_pend = (long long)ld_cg_u64(&F0->pend_n);
+#pragma unroll
+      for (int b2 = 0; b2 < 3; ++b2) sm.bins[b2] = ld_cg_u64(&F0->bin[b2]);
+      sm.pend_next = pn;
       int s = -1;
       if (n_f > 0) {
         vis_n += n_f;
         vis_m += m_f;
-        const long long pn = (long long)ld_cg_u64(&F1->pend_n);
-        const long long pm = (long long)ld_cg_u64(&F1->pend_m);
+        if (blockIdx.x == 0) {
+          st_reached += n_f;
+          st_msum += m_f;
+          st_async += own_pend;
+        }
         long long n_u = p.n_ni - vis_n - pn;
         long long m_u = p.E - vis_m - pm;
         if (n_u < 0) n_u = 0;
         if (m_u < 0) m_u = 0;
         switch (p.policy) {
           case XBFS_POLICY_FORCED: {
-            long long i = L < p.n_forced ? L : p.n_forced - 1;
+            const long long i = L < p.n_forced ? L : p.n_forced - 1;
             s = (i >= 0) ? (int)p.forced[i] : XBFS_TD_QUEUE;
             if (s < 0 || s > 2) s = XBFS_TD_QUEUE;
             break;
@@ -657,7 +839,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         }
         if (s == XBFS_BU && !p.allow_bu) s = XBFS_TD_QUEUE;
         if (s == -2) {
-          // features are stored for warp 0
           sm.mlp_h[0][0] = flog((double)n_f);
           sm.mlp_h[0][1] = flog((double)m_f);
           sm.mlp_h[0][2] = flog((double)n_u);
@@ -699,16 +880,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       ps.prev_strategy = S;
       if (blockIdx.x == 0) {
         if (L < p.hist_cap) p.hist[L].strategy = S;
-        ctl->strat_count[S] += 1;
-        ctl->reached += ld_cg_u64(&F0->n);
-        ctl->msum += ld_cg_u64(&F0->m);
-        ctl->n_async += ld_cg_u64(&F0->pend_n);
+        st_strat[S] += 1;
+        // counters used at level L+1 (last used at level L-1)
+        ctl->heavy[(L + 1) & 1] = 0ull;
+        ctl->bu_chunk[(L + 1) & 1] = 0u;
       }
     }
     // ---- housekeeping for slots no longer in use (first phase of the level)
-    if (blockIdx.x == 0 && threadIdx.x < 8) {
-      reinterpret_cast<unsigned long long*>(F3)[threadIdx.x] = 0ull;
-    }
+    if (blockIdx.x == 0 && threadIdx.x < 8) reinterpret_cast<unsigned long long*>(F3)[threadIdx.x] = 0ull;
     const int c3 = (int)((L + 3) & 3);
     if (dirty & (1u << c3)) {
       clear_bitmap(p.fb[c3], p.nwords);
@@ -720,31 +899,32 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
     const int par = (int)(L & 1);
 
     if (S == XBFS_TD_QUEUE || S == XBFS_TD_SCAN) {
-      if (!q_valid) {
-        QOut qs;
-        for (int b2 = 0; b2 < 3; ++b2) {
-          qs.ids[b2] = p.qids[par][b2];
-          qs.eb[b2] = p.qeb[par][b2];
-        }
-        qs.ctr = F0->bin;
-        sweep_bitmap_to_queue(p, sm, qs, fbc);
-        if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
-      }
-      const bool enq = (S == XBFS_TD_QUEUE) && (ld_cg_u64(&F1->pend_n) == 0);
+      const bool enq = (S == XBFS_TD_QUEUE) && (sm.pend_next == 0);
       QOut qo;
-      for (int b2 = 0; b2 < 3; ++b2) {
-        qo.ids[b2] = p.qids[par ^ 1][b2];
-        qo.eb[b2] = p.qeb[par ^ 1][b2];
-      }
+      for (int b2 = 0; b2 < 3; ++b2) qo.b[b2] = p.q[par ^ 1][b2];
       qo.ctr = F1->bin;
-      for (int bin = 2; bin >= 0; --bin) {
-        const unsigned long long pk = ld_cg_u64(&F0->bin[bin]);
-        gather_bin<PAR>(p, sm, qo, acc, p.qids[par][bin], p.qeb[par][bin], (unsigned)(pk & kCountMask),
-                        pk >> 31, (int)L, enq, fbn);
+      if (q_valid) {
+        for (int bin = 2; bin >= 0; --bin) {
+          const unsigned long long pk = sm.bins[bin];
+          gather_bin<PAR>(p, sm, qo, acc, p.q[par][bin], (unsigned)(pk & kCountMask), pk >> 31, (int)L, enq, fbn);
+        }
+      } else {
+        expand_bitmap<PAR>(p, sm, qo, acc, fbc, (int)L, enq, fbn, par);
       }
       if (enq) flush(sm, qo);
       publish_acc(sm, acc, F1, nullptr);
-      if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
+      if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+      if (!q_valid) {
+        // heavy vertices deferred by the fused sweep: expand them grid-wide
+        // (the list is complete only after the barrier; usually it is empty)
+        const unsigned long long hk = ld_cg_u64(&ctl->heavy[par]);
+        if ((hk & kCountMask) != 0) {
+          gather_bin<PAR>(p, sm, qo, acc, p.heavy, (unsigned)(hk & kCountMask), hk >> 31, (int)L, enq, fbn);
+          if (enq) flush(sm, qo);
+          publish_acc(sm, acc, F1, nullptr);
+          if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+        }
+      }
       q_valid = enq;
       b_valid = !enq;
       if (!enq) dirty |= 1u << ((L + 1) & 3);
@@ -752,14 +932,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       if (!b_valid) {
         scatter_queue_to_bitmap(p, par, *F0, fbc);
         dirty |= 1u << (L & 3);
-        if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
+        if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
       }
       if (p.async_bu)
         bottom_up<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
       else
         bottom_up<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
       publish_acc(sm, acc, F1, F2);
-      if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
+      if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
       q_valid = false;
       b_valid = true;
       dirty |= 1u << ((L + 1) & 3);
@@ -768,6 +948,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     ctl->depth = (int)L;
+    // a stepped launch adds its levels to what earlier launches counted
+    ctl->reached += st_reached;
+    ctl->msum += st_msum;
+    ctl->n_async += st_async;
+    for (int k = 0; k < 3; ++k) ctl->strat_count[k] += st_strat[k];
     if (L > 0 && L - 1 < p.hist_cap) p.hist[L - 1].t1 = globaltimer_ns();
   }
 }
@@ -781,14 +966,16 @@ __global__ void k_seed(Params p, int src, int par_enabled) {
   const uint32_t word = (uint32_t)src >> 5, bit = 1u << (src & 31);
   p.vis[word] |= bit;
   p.fb[0][word] |= bit;
-  const long long d = p.beg[src + 1] - p.beg[src];
+  const long long b0 = p.beg[src];
+  const long long d = p.beg[src + 1] - b0;
   FDesc& f = p.ctl->fd[0];
   f.n = 1;
   f.m = (unsigned long long)d;
   if (d > 0) {
     const int bin = bin_of(d, p.small_max, p.medium_max);
-    p.qids[0][bin][0] = src;
-    p.qeb[0][bin][0] = 0;
+    p.q[0][bin].ids[0] = src;
+    p.q[0][bin].eb[0] = 0;
+    p.q[0][bin].bg[0] = b0;
     f.bin[bin] = ((unsigned long long)d << 31) | 1ull;
   }
 }
@@ -804,10 +991,15 @@ static xbfs_status ensure_workspace(Graph* g, int small_max, int medium_max) {
     w.V = g->V;
     w.nwords = (size_t)nwords;
     if ((st = w.bits.ensure((size_t)nwords * 4 * 5))) return st;
-    if ((st = w.ulist.ensure((size_t)nwords * 32 * 4))) return st;
     if ((st = w.ctl.ensure(sizeof(Ctl)))) return st;
+    if ((st = w.rs.ensure(sizeof(ResumeState)))) return st;
     w.hist_cap = 1 << 16;
     if ((st = w.hist.ensure(sizeof(LevelRecDev) * (size_t)w.hist_cap))) return st;
+    // heavy list of the fused sweep: vertices with degree > kHeavyDeg (<= degree > 16)
+    const size_t hcap = (size_t)g->cnt_deg_gt[4] + 1;
+    if ((st = w.heavy_ids.ensure(hcap * 4)) || (st = w.heavy_eb.ensure(hcap * 4)) ||
+        (st = w.heavy_bg.ensure(hcap * 8)))
+      return st;
     XBFS_CUDA_TRY(cudaEventCreate(&w.ev0));
     XBFS_CUDA_TRY(cudaEventCreate(&w.ev1));
     XBFS_CUDA_TRY(cudaEventCreate(&w.evk0));
@@ -815,7 +1007,6 @@ static xbfs_status ensure_workspace(Graph* g, int small_max, int medium_max) {
   }
   // queue capacities per bin: vertices with degree in the bin's range
   auto count_gt = [&](long long t) -> size_t {
-    // vertices with degree > t, upper bound from the power-of-two histogram
     if (t < 1) return (size_t)g->V;
     int k = 0;
     while (k < 15 && (1ll << (k + 1)) <= t) ++k;
@@ -830,10 +1021,92 @@ static xbfs_status ensure_workspace(Graph* g, int small_max, int medium_max) {
       for (int par = 0; par < 2; ++par) {
         if ((st = w.qids[par][b].ensure((cap[b] + 1) * 4))) return st;
         if ((st = w.qeb[par][b].ensure((cap[b] + 1) * 4))) return st;
+        if ((st = w.qbg[par][b].ensure((cap[b] + 1) * 8))) return st;
       }
       w.qcap[b] = cap[b] + 1;
     }
   }
+  return XBFS_OK;
+}
+
+// Fills the kernel parameters for one traversal of g with options o.
+static xbfs_status setup_params(Graph* g, const xbfs_opts& o, int* d_levels, int* d_parents, Params& p,
+                                const void** kfn_out, size_t* smem_out, int* grid_out) {
+  SsWorkspace& w = g->ss;
+  memset(&p, 0, sizeof(p));
+  p.beg = g->beg.as<long long>();
+  p.csr = g->csr.as<int>();
+  p.V = g->V;
+  p.E = g->E;
+  p.levels = d_levels;
+  p.parents = d_parents;
+  uint32_t* bits = w.bits.as<uint32_t>();
+  p.vis = bits;
+  for (int i = 0; i < 4; ++i) p.fb[i] = bits + (size_t)(i + 1) * w.nwords;
+  for (int par = 0; par < 2; ++par)
+    for (int b = 0; b < 3; ++b) {
+      p.q[par][b].ids = w.qids[par][b].as<int>();
+      p.q[par][b].eb = w.qeb[par][b].as<unsigned>();
+      p.q[par][b].bg = w.qbg[par][b].as<long long>();
+    }
+  p.heavy.ids = w.heavy_ids.as<int>();
+  p.heavy.eb = w.heavy_eb.as<unsigned>();
+  p.heavy.bg = w.heavy_bg.as<long long>();
+  p.ctl = w.ctl.as<Ctl>();
+  p.hist = w.hist.as<LevelRecDev>();
+  p.hist_cap = w.hist_cap;
+  p.forced = w.forced.as<signed char>();
+  p.n_forced = o.n_forced;
+  p.nwords = (g->V + 31) / 32;
+  p.n_ni = g->symmetric ? g->V - g->n_isolated : g->V;
+  p.policy = o.policy;
+  p.alpha = o.alpha;
+  p.async_bu = o.async_bu ? 1 : 0;
+  p.small_max = o.small_max;
+  p.medium_max = o.medium_max;
+  p.beamer_alpha = o.beamer_alpha > 0 ? o.beamer_alpha : 14.f;
+  p.beamer_beta = o.beamer_beta > 0 ? o.beamer_beta : 24.f;
+  p.timeout_ns = 10ull * 1000 * 1000 * 1000;
+  p.max_levels = g->V + 2;
+  extern const float* mlp_device_weights(int device);
+  p.mlp = mlp_device_weights(g->device);
+  if (o.policy == XBFS_POLICY_MLP && !p.mlp) p.policy = XBFS_POLICY_HEURISTIC;
+  p.allow_bu = g->symmetric ? 1 : 0;
+
+  const bool par_on = d_parents != nullptr;
+  const void* kfn = par_on ? (const void*)k_bfs<true> : (const void*)k_bfs<false>;
+  const size_t smem = sizeof(Smem);
+  XBFS_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int nsm = 0, per_sm = 0;
+  XBFS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device));
+  XBFS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kBlock, smem));
+  if (per_sm < 1) return set_error(XBFS_ERR_INTERNAL, "traversal kernel cannot be resident");
+  int grid = nsm * per_sm;
+  if (o.grid_dim > 0 && o.grid_dim < grid) grid = o.grid_dim;
+  w.grid = grid;
+  w.block = kBlock;
+  p.rs = w.rs.as<ResumeState>();
+  p.bu_mode = o.reserved[0];
+  p.stop_level = LLONG_MAX;
+  p.resume = 0;
+  *kfn_out = kfn;
+  *smem_out = smem;
+  *grid_out = grid;
+  return XBFS_OK;
+
+}
+
+// Initial state of a traversal from src: levels/parents -1, visited = isolated
+// vertices, frontier bitmaps and control block cleared, source seeded.
+static xbfs_status init_state(Graph* g, const Params& p, int src, bool par_on, cudaStream_t s) {
+  SsWorkspace& w = g->ss;
+  XBFS_CUDA_TRY(cudaMemsetAsync(p.levels, 0xff, (size_t)g->V * 4, s));
+  if (par_on) XBFS_CUDA_TRY(cudaMemsetAsync(p.parents, 0xff, (size_t)g->V * 4, s));
+  XBFS_CUDA_TRY(cudaMemcpyAsync(p.vis, g->iso.p, w.nwords * 4, cudaMemcpyDeviceToDevice, s));
+  XBFS_CUDA_TRY(cudaMemsetAsync(p.fb[0], 0, w.nwords * 4 * 4, s));
+  XBFS_CUDA_TRY(cudaMemsetAsync(p.ctl, 0, sizeof(Ctl), s));
+  k_seed<<<1, 32, 0, s>>>(p, src, par_on ? 1 : 0);
+  XBFS_CUDA_TRY(cudaGetLastError());
   return XBFS_OK;
 }
 
@@ -892,65 +1165,15 @@ xbfs_status bfs_single(Graph* g, int32_t src, int32_t* levels, int32_t* parents,
   }
 
   Params p;
-  memset(&p, 0, sizeof(p));
-  p.beg = g->beg.as<long long>();
-  p.csr = g->csr.as<int>();
-  p.V = g->V;
-  p.E = g->E;
-  p.levels = d_levels;
-  p.parents = d_parents;
-  uint32_t* bits = w.bits.as<uint32_t>();
-  p.vis = bits;
-  for (int i = 0; i < 4; ++i) p.fb[i] = bits + (size_t)(i + 1) * w.nwords;
-  for (int par = 0; par < 2; ++par)
-    for (int b = 0; b < 3; ++b) {
-      p.qids[par][b] = w.qids[par][b].as<int>();
-      p.qeb[par][b] = w.qeb[par][b].as<unsigned>();
-    }
-  p.ulist = w.ulist.as<int>();
-  p.ctl = w.ctl.as<Ctl>();
-  p.hist = w.hist.as<LevelRecDev>();
-  p.hist_cap = w.hist_cap;
-  p.forced = w.forced.as<signed char>();
-  p.n_forced = o.n_forced;
-  p.nwords = (g->V + 31) / 32;
-  p.n_ni = g->symmetric ? g->V - g->n_isolated : g->V;
-  p.policy = o.policy;
-  p.alpha = o.alpha;
-  p.async_bu = o.async_bu ? 1 : 0;
-  p.small_max = o.small_max;
-  p.medium_max = o.medium_max;
-  p.beamer_alpha = o.beamer_alpha > 0 ? o.beamer_alpha : 14.f;
-  p.beamer_beta = o.beamer_beta > 0 ? o.beamer_beta : 24.f;
-  p.timeout_ns = 10ull * 1000 * 1000 * 1000;
-  p.max_levels = g->V + 2;
-  extern const float* mlp_device_weights(int device);
-  p.mlp = mlp_device_weights(g->device);
-  if (o.policy == XBFS_POLICY_MLP && !p.mlp) p.policy = XBFS_POLICY_HEURISTIC;
-  p.allow_bu = g->symmetric ? 1 : 0;
-
+  const void* kfn = nullptr;
+  size_t smem = 0;
+  int grid = 0;
+  if ((st = setup_params(g, o, d_levels, d_parents, p, &kfn, &smem, &grid))) return st;
   const bool par_on = parents != nullptr;
-  const void* kfn = par_on ? (const void*)k_bfs<true> : (const void*)k_bfs<false>;
-  const size_t smem = sizeof(Smem);
-  XBFS_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int nsm = 0, per_sm = 0;
-  XBFS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device));
-  XBFS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kBlock, smem));
-  if (per_sm < 1) return set_error(XBFS_ERR_INTERNAL, "traversal kernel cannot be resident");
-  int grid = nsm * per_sm;
-  if (o.grid_dim > 0 && o.grid_dim < grid) grid = o.grid_dim;
-  w.grid = grid;
-  w.block = kBlock;
 
   // ---- initial state
   XBFS_CUDA_TRY(cudaEventRecord(w.ev0, s));
-  XBFS_CUDA_TRY(cudaMemsetAsync(d_levels, 0xff, (size_t)g->V * 4, s));
-  if (par_on) XBFS_CUDA_TRY(cudaMemsetAsync(d_parents, 0xff, (size_t)g->V * 4, s));
-  XBFS_CUDA_TRY(cudaMemcpyAsync(p.vis, g->iso.p, w.nwords * 4, cudaMemcpyDeviceToDevice, s));
-  XBFS_CUDA_TRY(cudaMemsetAsync(p.fb[0], 0, w.nwords * 4 * 4, s));
-  XBFS_CUDA_TRY(cudaMemsetAsync(p.ctl, 0, sizeof(Ctl), s));
-  k_seed<<<1, 32, 0, s>>>(p, src, par_on ? 1 : 0);
-  XBFS_CUDA_TRY(cudaGetLastError());
+  if ((st = init_state(g, p, src, par_on, s))) return st;
   void* args[] = {&p};
   XBFS_CUDA_TRY(cudaEventRecord(w.evk0, s));
   XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, smem, s));
@@ -1000,6 +1223,121 @@ xbfs_status bfs_single(Graph* g, int32_t src, int32_t* levels, int32_t* parents,
   return XBFS_OK;
 }
 
+// Per-level strategy costs for training the learned switch: at every level
+// the whole traversal state is snapshotted, the level is run once with each
+// strategy from that snapshot (one stepped launch each, timed with the
+// device's globaltimer between the level's start and its closing barrier),
+// and the traversal continues along the cheapest strategy (follow = 0) or
+// the reference heuristic's choice (follow = 1).
+xbfs_status level_costs(Graph* g, int32_t src, int32_t follow, int32_t cap, float* costs, xbfs_level_trace* trace,
+                        int32_t* n_out) {
+  if (!g || !costs || !trace || !n_out || cap <= 0) return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
+  if (src < 0 || (int64_t)src >= g->V) return set_error(XBFS_ERR_INVALID_ARG, "source out of range");
+  if (g->E >= (1ll << 32)) return set_error(XBFS_ERR_UNSUPPORTED, "needs E < 2^32");
+  xbfs_opts o;
+  xbfs_opts_init(&o);
+  DeviceGuard dg(g->device);
+  xbfs_status st = ensure_workspace(g, o.small_max, o.medium_max);
+  if (st) return st;
+  SsWorkspace& w = g->ss;
+  cudaStream_t s = g->stream;
+  if ((st = w.levels_tmp.ensure((size_t)g->V * 4))) return st;
+  if (cap + 1 > w.forced_cap) {
+    if ((st = w.forced.ensure((size_t)cap + 1))) return st;
+    w.forced_cap = cap + 1;
+  }
+  std::vector<signed char> forced((size_t)cap + 1, 0);
+  o.policy = XBFS_POLICY_FORCED;
+  o.forced = (const int8_t*)forced.data();
+  o.n_forced = cap + 1;
+  Params p;
+  const void* kfn = nullptr;
+  size_t smem = 0;
+  int grid = 0;
+  if ((st = setup_params(g, o, w.levels_tmp.as<int>(), nullptr, p, &kfn, &smem, &grid))) return st;
+  // snapshot layout: levels | bitmaps | queues (2 parities x 3 bins) | ctl | resume state
+  struct Piece { void* p; size_t n; };
+  std::vector<Piece> pieces;
+  pieces.push_back({w.levels_tmp.p, (size_t)g->V * 4});
+  pieces.push_back({w.bits.p, w.nwords * 4 * 5});
+  for (int par = 0; par < 2; ++par)
+    for (int b = 0; b < 3; ++b) {
+      pieces.push_back({w.qids[par][b].p, w.qcap[b] * 4});
+      pieces.push_back({w.qeb[par][b].p, w.qcap[b] * 4});
+      pieces.push_back({w.qbg[par][b].p, w.qcap[b] * 8});
+    }
+  pieces.push_back({w.ctl.p, sizeof(Ctl)});
+  pieces.push_back({w.rs.p, sizeof(ResumeState)});
+  size_t total = 0;
+  for (auto& pc : pieces) total += (pc.n + 255) & ~(size_t)255;
+  if ((st = w.snap.ensure(total))) return st;
+  auto copy_all = [&](bool save) -> xbfs_status {
+    size_t off = 0;
+    for (auto& pc : pieces) {
+      char* sp = w.snap.as<char>() + off;
+      XBFS_CUDA_TRY(cudaMemcpyAsync(save ? sp : pc.p, save ? pc.p : sp, pc.n, cudaMemcpyDeviceToDevice, s));
+      off += (pc.n + 255) & ~(size_t)255;
+    }
+    return XBFS_OK;
+  };
+  auto run_level = [&](int L, int strategy, int policy, LevelRecDev* rec) -> xbfs_status {
+    forced[L] = (signed char)strategy;
+    XBFS_CUDA_TRY(cudaMemcpyAsync(w.forced.p, forced.data(), (size_t)L + 1, cudaMemcpyHostToDevice, s));
+    XBFS_CUDA_TRY(cudaMemsetAsync(p.ctl, 0, sizeof(GridBarrier), s));  // fresh barrier epoch
+    Params q = p;
+    q.policy = policy;
+    q.resume = L > 0 ? 1 : 0;
+    q.stop_level = L + 1;
+    void* args[] = {&q};
+    XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, smem, s));
+    XBFS_CUDA_TRY(cudaMemcpyAsync(rec, p.hist + L, sizeof(LevelRecDev), cudaMemcpyDeviceToHost, s));
+    int err = 0;
+    XBFS_CUDA_TRY(cudaMemcpyAsync(&err, &p.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    XBFS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (err) return set_error((xbfs_status)err, "stepped traversal reported %s", xbfs_strerror(err));
+    return XBFS_OK;
+  };
+  if ((st = init_state(g, p, src, false, s))) return st;
+  int n = 0;
+  for (int L = 0; L < cap; ++L) {
+    // is there a level-L frontier?
+    FDesc f;
+    XBFS_CUDA_TRY(cudaMemcpyAsync(&f, &p.ctl->fd[L & 3], sizeof(FDesc), cudaMemcpyDeviceToHost, s));
+    XBFS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (f.n == 0) break;
+    if ((st = copy_all(true))) return st;
+    LevelRecDev rec[3];
+    for (int k = 0; k < 3; ++k) {
+      if (k > 0 && (st = copy_all(false))) return st;
+      if ((st = run_level(L, k, XBFS_POLICY_FORCED, &rec[k]))) return st;
+      costs[L * 3 + k] = (rec[k].t1 > rec[k].t0) ? (float)((rec[k].t1 - rec[k].t0) * 1e-3) : 0.f;
+    }
+    int choice = 0;
+    if (follow == 1) {
+      LevelRecDev hr;
+      if ((st = copy_all(false))) return st;
+      if ((st = run_level(L, 0, XBFS_POLICY_HEURISTIC, &hr))) return st;
+      choice = hr.strategy;
+    } else {
+      for (int k = 1; k < 3; ++k)
+        if (costs[L * 3 + k] < costs[L * 3 + choice]) choice = k;
+    }
+    if ((st = copy_all(false))) return st;
+    LevelRecDev cr;
+    if ((st = run_level(L, choice, XBFS_POLICY_FORCED, &cr))) return st;
+    trace[L].level = L;
+    trace[L].strategy = cr.strategy;
+    trace[L].n_f = cr.n_f;
+    trace[L].m_f = cr.m_f;
+    trace[L].n_u = cr.n_u;
+    trace[L].m_u = cr.m_u;
+    trace[L].us = (cr.t1 > cr.t0) ? (double)(cr.t1 - cr.t0) * 1e-3 : 0.0;
+    n = L + 1;
+  }
+  *n_out = n;
+  return XBFS_OK;
+}
+
 }  // namespace xbfs
 
 using namespace xbfs;
@@ -1009,6 +1347,11 @@ extern "C" {
 xbfs_status xbfs_bfs(xbfs_graph* gh, int32_t src, int32_t* levels, int32_t* parents, const xbfs_opts* opts,
                      xbfs_stats* stats) {
   return bfs_single((Graph*)gh, src, levels, parents, opts, stats);
+}
+
+xbfs_status xbfs_level_costs(xbfs_graph* gh, int32_t src, int32_t follow, int32_t cap, float* costs,
+                             xbfs_level_trace* trace, int32_t* n) {
+  return level_costs((Graph*)gh, src, follow, cap, costs, trace, n);
 }
 
 xbfs_status xbfs_last_trace(xbfs_graph* gh, xbfs_level_trace* out, int32_t cap, int32_t* n) {

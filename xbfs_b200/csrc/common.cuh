@@ -88,36 +88,41 @@ __device__ __forceinline__ long long ld_nc_i64(const long long* p) {
 // hanging. Any block that sees a non-zero error word also leaves.
 // ---------------------------------------------------------------------------
 struct GridBarrier {
-  uint32_t count;
-  uint32_t gen;
+  uint32_t count;  // arrivals since launch (zeroed before the launch)
+  uint32_t pad;
 };
 
-__device__ __forceinline__ bool grid_sync(GridBarrier* bar, uint32_t nblocks, int* err,
+// Count-up barrier: the k-th barrier of a launch completes when `count`
+// reaches k * nblocks. One release-add per CTA, no reset and no generation
+// flip on the critical path; `epoch` is the CTA's own count of barriers
+// passed (identical in all CTAs). 2^32 arrivals allow > 10^7 barriers at
+// 296 CTAs.
+__device__ __forceinline__ void red_add_release_u32(uint32_t* p, uint32_t v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar, uint32_t nblocks, uint32_t& epoch, int* err,
                                           unsigned long long timeout_ns) {
   __shared__ int s_ok;
   __syncthreads();
+  epoch += 1;
   if (threadIdx.x == 0) {
     int ok = 1;
-    const uint32_t g = ld_acquire_u32(&bar->gen);
+    const uint32_t target = epoch * nblocks;
     __threadfence();
-    const uint32_t prev = atomicAdd(&bar->count, 1u);
-    if (prev == nblocks - 1) {
-      atomicExch(&bar->count, 0u);
-      __threadfence();
-      atomicAdd(&bar->gen, 1u);
-    } else {
-      const unsigned long long t0 = globaltimer_ns();
-      uint32_t spins = 0;
-      while (ld_acquire_u32(&bar->gen) == g) {
-        ++spins;
-        if (spins > 256) __nanosleep(64);
-        if ((spins & 255u) == 0) {
-          if (ld_acquire_i32(err) != 0) { ok = 0; break; }
-          if (globaltimer_ns() - t0 > timeout_ns) {
-            atomicCAS(err, 0, (int)XBFS_ERR_DEVICE_TIMEOUT);
-            ok = 0;
-            break;
-          }
+    red_add_release_u32(&bar->count, 1u);
+    uint32_t spins = 0;
+    unsigned long long t0 = 0;
+    while ((int32_t)(ld_acquire_u32(&bar->count) - target) < 0) {
+      ++spins;
+      if (spins > 2048) __nanosleep(32);
+      if ((spins & 1023u) == 0) {
+        if (t0 == 0) t0 = globaltimer_ns();
+        if (ld_acquire_i32(err) != 0) { ok = 0; break; }
+        if (globaltimer_ns() - t0 > timeout_ns) {
+          atomicCAS(err, 0, (int)XBFS_ERR_DEVICE_TIMEOUT);
+          ok = 0;
+          break;
         }
       }
     }
@@ -169,6 +174,28 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T* total) {
   *total = s_warp[NW];
   __syncthreads();
   return res;
+}
+
+// Sums N values per thread over the block in one pass (two barriers).
+// `s` needs N * (BLOCK/32) slots; every thread receives all N totals.
+template <int BLOCK, int N, typename T>
+__device__ __forceinline__ void block_sum_n(T (&v)[N], T* s) {
+  constexpr int NW = BLOCK / 32;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const T t = warp_sum(v[k]);
+    if (lane == 0) s[k * NW + wid] = t;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    T t = 0;
+#pragma unroll
+    for (int i = 0; i < NW; ++i) t += s[k * NW + i];
+    v[k] = t;
+  }
+  __syncthreads();
 }
 
 template <int BLOCK, typename T>

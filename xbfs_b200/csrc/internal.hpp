@@ -52,11 +52,12 @@ struct SsWorkspace {
   DevBuf bits;             // vis + 4 frontier bitmaps, contiguous
   DevBuf qids[2][3];       // per parity, per bin: vertex ids
   DevBuf qeb[2][3];        // per parity, per bin: edge offsets (uint32)
+  DevBuf qbg[2][3];        // per parity, per bin: CSR offsets (int64)
   size_t qcap[3] = {0, 0, 0};
-  DevBuf ulist;            // bottom-up list of unvisited vertices
-  DevBuf scan_st;          // 2 x ntiles tile descriptors for the ordered scan
-  size_t ntiles = 0;
+  DevBuf heavy_ids, heavy_eb, heavy_bg;  // heavy vertices deferred by a fused sweep
   DevBuf ctl;              // control block
+  DevBuf rs;               // loop state of a stepped traversal
+  DevBuf snap;             // snapshot of the whole traversal state (stepped mode)
   DevBuf hist;             // per-level records
   int hist_cap = 0;
   DevBuf forced;           // int8 per-level strategies

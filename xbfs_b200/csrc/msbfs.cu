@@ -32,6 +32,7 @@ namespace ms {
 
 constexpr int kBlock = 512;
 constexpr int kTE = kBlock;  // edges per gather round
+constexpr int kMsLight = 64;  // bottom-up: larger degrees are pulled edge-balanced
 constexpr unsigned long long kCountMask = (1ull << 31) - 1;
 
 struct Ctl {
@@ -42,6 +43,7 @@ struct Ctl {
   unsigned int tcount[2];         // touched-list length by level parity
   unsigned long long m_done[3];   // degree sum of vertices completed, per level ring
   unsigned long long n_done[3];
+  unsigned long long heavy[2];    // packed counter of the bottom-up heavy list, by level parity
   int strat_count[2];
 };
 
@@ -60,6 +62,8 @@ struct Params {
   unsigned* qeb[3];
   int* tlist;
   int* ulist;
+  int* hq_ids;              // bottom-up heavy list
+  unsigned* hq_eb;
   Ctl* ctl;
   unsigned long long full[W];
   long long nwords;
@@ -143,6 +147,138 @@ __device__ __forceinline__ void complete_vertex(const Params<W, RowT>& p, int v,
   }
 }
 
+// Edge-balanced pass over a queue (ids + exclusive edge offsets). PULL =
+// false: top-down, the owner's frontier bits are pushed into each
+// neighbour's accumulator. PULL = true: bottom-up for heavy vertices, each
+// neighbour's frontier bits are pulled into the owner's accumulator. Every
+// vertex whose accumulator gains bits is appended once to the touched list.
+template <int W, typename RowT, bool PULL>
+__device__ void ms_gather(const Params<W, RowT>& p, Smem& sm, const int* ids, const unsigned* eb, unsigned cnt,
+                          unsigned long long M, const unsigned long long* Fc, unsigned* tctr) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long nb = gridDim.x;
+  const unsigned long long lo = M * blockIdx.x / nb, hi = M * (blockIdx.x + 1) / nb;
+  if (cnt == 0 || lo >= hi) return;
+  if (threadIdx.x < 32) {
+    unsigned a = 0, b = cnt;
+    while (b - a > 32) {
+      const unsigned span = b - a;
+      const unsigned piv = a + (unsigned)(((unsigned long long)span * lane) / 32);
+      const unsigned m = __ballot_sync(0xffffffffu, (unsigned long long)eb[piv] <= lo);
+      const int last = 31 - __clz(m);
+      const unsigned na = a + (unsigned)(((unsigned long long)span * last) / 32);
+      const unsigned nbb = (last == 31) ? b : a + (unsigned)(((unsigned long long)span * (last + 1)) / 32);
+      a = na;
+      b = nbb;
+    }
+    const unsigned idx = a + lane;
+    const unsigned m = __ballot_sync(0xffffffffu, idx < b && (unsigned long long)eb[idx] <= lo);
+    if (lane == 0) sm.next_s = (int)(a + 31 - __clz(m));
+  }
+  __syncthreads();
+  unsigned s = (unsigned)sm.next_s;
+  for (unsigned long long r = lo; r < hi; r += kTE) {
+    const unsigned long long rhi = (r + kTE < hi) ? r + kTE : hi;
+    for (int i = threadIdx.x; i <= kTE; i += kBlock) {
+      const unsigned slot = s + (unsigned)i;
+      unsigned e0 = 0xffffffffu;
+      if (slot < cnt) {
+        const unsigned x = eb[slot];
+        if ((unsigned long long)x < rhi) {
+          e0 = x;
+          const int u = ids[slot];
+          sm.wu[i] = u;
+          sm.wbeg[i] = ld_nc_i64(p.beg + u);
+        }
+      }
+      sm.web[i] = e0;
+    }
+    __syncthreads();
+    const unsigned long long e = r + threadIdx.x;
+    bool first = false;
+    int dst = 0;
+    if (e < rhi) {
+      int a = 0, c = kTE + 1;
+      while (c - a > 1) {
+        const int mid = (a + c) >> 1;
+        if ((unsigned long long)sm.web[mid] <= e) a = mid; else c = mid;
+      }
+      const int owner = sm.wu[a];
+      const int nbr = ld_stream_i32(p.csr + sm.wbeg[a] + (long long)(e - sm.web[a]));
+      const int src = PULL ? nbr : owner;
+      dst = PULL ? owner : nbr;
+      bool any = false;
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        const unsigned long long f = Fc[(size_t)src * W + w];
+        if (!f) continue;
+        unsigned long long m = f & ~ld_cg_u64(p.vis + (size_t)dst * W + w);
+        if (PULL) m &= p.full[w];
+        if (m) {
+          red_or_u64(p.N + (size_t)dst * W + w, m);
+          any = true;
+        }
+      }
+      if (any) {
+        const uint32_t bit = 1u << (dst & 31);
+        if (!(ld_cg_u32(p.touched + (dst >> 5)) & bit)) {
+          const uint32_t old = atomicOr(p.touched + (dst >> 5), bit);
+          first = !(old & bit);
+        }
+      }
+    }
+    const unsigned tm = __ballot_sync(0xffffffffu, first);
+    if (tm) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(tctr, (unsigned)__popc(tm));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (first) p.tlist[base + __popc(tm & ((1u << lane) - 1))] = dst;
+    }
+    if (threadIdx.x == 0 && rhi < hi) {
+      int a = 0, c = kTE + 1;
+      while (c - a > 1) {
+        const int mid = (a + c) >> 1;
+        if ((unsigned long long)sm.web[mid] <= rhi) a = mid; else c = mid;
+      }
+      sm.next_s = (int)(s + a);
+    }
+    __syncthreads();
+    s = (unsigned)sm.next_s;
+  }
+}
+
+// Merge the accumulators of the touched vertices into visited / next frontier,
+// record their levels and queue the ones that gained bits.
+template <int W, typename RowT>
+__device__ void ms_merge(const Params<W, RowT>& p, long long L, unsigned long long* Fn, int* qout, unsigned* qeb_out,
+                         unsigned long long* qctr, long long& m_done, long long& n_done) {
+  const unsigned tc = ld_cg_u32(&p.ctl->tcount[L & 1]);
+  const long long nth = (long long)gridDim.x * kBlock;
+  for (long long i0 = blockIdx.x * (long long)kBlock; i0 < tc; i0 += nth) {
+    const long long i = i0 + threadIdx.x;
+    bool have = false;
+    int v = 0;
+    long long deg = 0;
+    if (i < tc) {
+      v = p.tlist[i];
+      p.touched[v >> 5] = 0u;  // every touched bit of this word is merged in this phase
+      unsigned long long nw[W], vn[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        const size_t k = (size_t)v * W + w;
+        const unsigned long long a = p.N[k];
+        const unsigned long long vv = p.vis[k];
+        if (a) p.N[k] = 0ull;
+        nw[w] = a & ~vv;
+        vn[w] = vv | nw[w];
+      }
+      deg = ld_nc_i64(p.beg + v + 1) - ld_nc_i64(p.beg + v);
+      complete_vertex<W, RowT>(p, v, nw, vn, (int)(L + 1), Fn, qout, qeb_out, qctr, deg, m_done, n_done, have);
+    }
+    warp_enqueue(qout, qeb_out, qctr, have && deg > 0, v, deg);
+  }
+}
+
 template <int W, typename RowT>
 __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, RowT> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -153,6 +289,7 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
   const long long gtid = blockIdx.x * (long long)kBlock + threadIdx.x;
   const long long nth = (long long)gridDim.x * kBlock;
   long long m_done_total = 0;  // thread 0 only
+  uint32_t epoch = 0;
   long long L = 0;
   for (;; ++L) {
     if (L >= p.max_levels) {
@@ -200,128 +337,19 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
       ctl->tcount[(L + 1) & 1] = 0;
       ctl->m_done[qn] = 0;
       ctl->n_done[qn] = 0;
+      ctl->heavy[(L + 1) & 1] = 0ull;
     }
     long long m_done = 0, n_done = 0;
     if (D == 0) {
-      // ---------------- top-down: edge-balanced gather over the frontier queue
-      const unsigned long long M = mf;
-      const unsigned long long lo = M * blockIdx.x / nb, hi = M * (blockIdx.x + 1) / nb;
-      unsigned* tctr = &ctl->tcount[L & 1];
-      if (lo < hi) {
-        if (threadIdx.x < 32) {
-          // last slot with eb <= lo
-          unsigned a = 0, b = cnt;
-          while (b - a > 32) {
-            const unsigned span = b - a;
-            const unsigned piv = a + (unsigned)(((unsigned long long)span * lane) / 32);
-            const unsigned m = __ballot_sync(0xffffffffu, (unsigned long long)qeb_in[piv] <= lo);
-            const int last = 31 - __clz(m);
-            const unsigned na = a + (unsigned)(((unsigned long long)span * last) / 32);
-            const unsigned nbb = (last == 31) ? b : a + (unsigned)(((unsigned long long)span * (last + 1)) / 32);
-            a = na;
-            b = nbb;
-          }
-          const unsigned idx = a + lane;
-          const unsigned m = __ballot_sync(0xffffffffu, idx < b && (unsigned long long)qeb_in[idx] <= lo);
-          if (lane == 0) sm.next_s = (int)(a + 31 - __clz(m));
-        }
-        __syncthreads();
-        unsigned s = (unsigned)sm.next_s;
-        for (unsigned long long r = lo; r < hi; r += kTE) {
-          const unsigned long long rhi = (r + kTE < hi) ? r + kTE : hi;
-          for (int i = threadIdx.x; i <= kTE; i += kBlock) {
-            const unsigned slot = s + (unsigned)i;
-            unsigned e0 = 0xffffffffu;
-            if (slot < cnt) {
-              const unsigned x = qeb_in[slot];
-              if ((unsigned long long)x < rhi) {
-                e0 = x;
-                const int u = qin[slot];
-                sm.wu[i] = u;
-                sm.wbeg[i] = ld_nc_i64(p.beg + u);
-              }
-            }
-            sm.web[i] = e0;
-          }
-          __syncthreads();
-          const unsigned long long e = r + threadIdx.x;
-          bool first = false;
-          int v = 0;
-          if (e < rhi) {
-            int a = 0, c = kTE + 1;
-            while (c - a > 1) {
-              const int mid = (a + c) >> 1;
-              if ((unsigned long long)sm.web[mid] <= e) a = mid; else c = mid;
-            }
-            const int u = sm.wu[a];
-            v = ld_stream_i32(p.csr + sm.wbeg[a] + (long long)(e - sm.web[a]));
-            bool any = false;
-#pragma unroll
-            for (int w = 0; w < W; ++w) {
-              const unsigned long long f = Fc[(size_t)u * W + w];
-              if (!f) continue;
-              const unsigned long long m = f & ~ld_cg_u64(p.vis + (size_t)v * W + w);
-              if (m) {
-                red_or_u64(p.N + (size_t)v * W + w, m);
-                any = true;
-              }
-            }
-            if (any) {
-              const uint32_t bit = 1u << (v & 31);
-              if (!(ld_cg_u32(p.touched + (v >> 5)) & bit)) {
-                const uint32_t old = atomicOr(p.touched + (v >> 5), bit);
-                first = !(old & bit);
-              }
-            }
-          }
-          // warp-aggregated append to the touched list
-          const unsigned tm = __ballot_sync(0xffffffffu, first);
-          if (tm) {
-            unsigned base = 0;
-            if (lane == 0) base = atomicAdd(tctr, (unsigned)__popc(tm));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (first) p.tlist[base + __popc(tm & ((1u << lane) - 1))] = v;
-          }
-          if (threadIdx.x == 0 && rhi < hi) {
-            int a = 0, c = kTE + 1;
-            while (c - a > 1) {
-              const int mid = (a + c) >> 1;
-              if ((unsigned long long)sm.web[mid] <= rhi) a = mid; else c = mid;
-            }
-            sm.next_s = (int)(s + a);
-          }
-          __syncthreads();
-          s = (unsigned)sm.next_s;
-        }
-      }
-      if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
-      // ---------------- merge the touched vertices
-      const unsigned tc = ld_cg_u32(&ctl->tcount[L & 1]);
-      for (long long i0 = blockIdx.x * (long long)kBlock; i0 < tc; i0 += nth) {
-        const long long i = i0 + threadIdx.x;
-        bool have = false;
-        int v = 0;
-        long long deg = 0;
-        if (i < tc) {
-          v = p.tlist[i];
-          p.touched[v >> 5] = 0u;  // every touched bit of this word is merged in this phase
-          unsigned long long nw[W], vn[W];
-#pragma unroll
-          for (int w = 0; w < W; ++w) {
-            const size_t k = (size_t)v * W + w;
-            const unsigned long long a = p.N[k];
-            const unsigned long long vv = p.vis[k];
-            if (a) p.N[k] = 0ull;
-            nw[w] = a & ~vv;
-            vn[w] = vv | nw[w];
-          }
-          deg = ld_nc_i64(p.beg + v + 1) - ld_nc_i64(p.beg + v);
-          complete_vertex<W, RowT>(p, v, nw, vn, (int)(L + 1), Fn, qout, qeb_out, qctr, deg, m_done, n_done, have);
-        }
-        warp_enqueue(qout, qeb_out, qctr, have && deg > 0, v, deg);
-      }
+      // ---------------- top-down: push along the edges of the frontier queue
+      ms_gather<W, RowT, false>(p, sm, qin, qeb_in, cnt, mf, Fc, &ctl->tcount[L & 1]);
+      if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+      ms_merge<W, RowT>(p, L, Fn, qout, qeb_out, qctr, m_done, n_done);
     } else {
-      // ---------------- bottom-up over this CTA's slice of not-complete vertices
+      // ---------------- bottom-up: light vertices search their neighbours
+      // (lane per vertex, early exit); heavy ones are queued and pulled
+      // edge-balanced by the whole grid after the barrier
+      unsigned long long* hctr = &ctl->heavy[L & 1];
       const long long nw_ = p.nwords;
       const long long w0 = nw_ * blockIdx.x / nb, w1 = nw_ * (blockIdx.x + 1) / nb;
       int* list = p.ulist + w0 * 32;
@@ -351,39 +379,59 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= n) break;
         const int i = base + lane;
-        bool have = false;
+        bool have = false, heavy = false;
         int v = 0;
-        long long deg = 0;
+        long long deg = 0, e0 = 0;
         if (i < n) {
           v = list[i];
-          unsigned long long need[W], acc[W], vv[W];
-          bool open = false;
-#pragma unroll
-          for (int w = 0; w < W; ++w) {
-            vv[w] = p.vis[(size_t)v * W + w];
-            need[w] = p.full[w] & ~vv[w];
-            acc[w] = 0;
-            open |= need[w] != 0;
-          }
-          const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
-          deg = e1 - e0;
-          for (long long e = e0; e < e1 && open; ++e) {
-            const int u = ld_stream_i32(p.csr + e);
-            open = false;
+          e0 = ld_nc_i64(p.beg + v);
+          deg = ld_nc_i64(p.beg + v + 1) - e0;
+          heavy = deg > kMsLight;
+          if (!heavy) {
+            unsigned long long need[W], acc[W], vv[W];
+            bool open = false;
 #pragma unroll
             for (int w = 0; w < W; ++w) {
-              if (need[w] != acc[w]) {
-                acc[w] |= Fc[(size_t)u * W + w] & need[w];
+              vv[w] = p.vis[(size_t)v * W + w];
+              need[w] = p.full[w] & ~vv[w];
+              acc[w] = 0;
+              open |= need[w] != 0;
+            }
+            const long long e1 = e0 + deg;
+            for (long long e = e0; e < e1 && open; e += 4) {
+              int u[4];
+#pragma unroll
+              for (int k = 0; k < 4; ++k) u[k] = (e + k < e1) ? __ldg(p.csr + e + k) : -1;
+#pragma unroll
+              for (int k = 0; k < 4; ++k)
+                if (u[k] >= 0) {
+#pragma unroll
+                  for (int w = 0; w < W; ++w) acc[w] |= Fc[(size_t)u[k] * W + w];
+                }
+              open = false;
+#pragma unroll
+              for (int w = 0; w < W; ++w) {
+                acc[w] &= need[w];
                 open |= need[w] != acc[w];
               }
             }
-          }
-          unsigned long long vn[W];
+            unsigned long long vn[W];
 #pragma unroll
-          for (int w = 0; w < W; ++w) vn[w] = vv[w] | acc[w];
-          complete_vertex<W, RowT>(p, v, acc, vn, (int)(L + 1), Fn, qout, qeb_out, qctr, deg, m_done, n_done, have);
+            for (int w = 0; w < W; ++w) vn[w] = vv[w] | acc[w];
+            complete_vertex<W, RowT>(p, v, acc, vn, (int)(L + 1), Fn, qout, qeb_out, qctr, deg, m_done, n_done,
+                                     have);
+          }
         }
         warp_enqueue(qout, qeb_out, qctr, have && deg > 0, v, deg);
+        warp_enqueue(p.hq_ids, p.hq_eb, hctr, heavy, v, deg);
+      }
+      if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+      const unsigned long long hk = ld_cg_u64(hctr);
+      if ((hk & kCountMask) != 0) {
+        ms_gather<W, RowT, true>(p, sm, p.hq_ids, p.hq_eb, (unsigned)(hk & kCountMask), hk >> 31, Fc,
+                                 &ctl->tcount[L & 1]);
+        if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+        ms_merge<W, RowT>(p, L, Fn, qout, qeb_out, qctr, m_done, n_done);
       }
     }
     // publish completion statistics of this level
@@ -395,7 +443,7 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
         if (nd) atomicAdd(&ctl->n_done[L % 3], (unsigned long long)nd);
       }
     }
-    if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
+    if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
     // retire frontier L: clear its F entries (nobody reads them any more)
     {
       unsigned long long* Fr = p.F[L & 1];
@@ -408,7 +456,7 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
     // sources of degree 0 are never queued and keep their F bits; no vertex has
     // them as a neighbour (bottom-up runs on symmetric graphs only), so they are
     // never read again
-    if (!grid_sync(&ctl->bar, nb, &ctl->err, p.timeout_ns)) break;
+    if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->depth = (int)L;
 }
@@ -490,7 +538,7 @@ __global__ void k_ms_transpose(const RowT* rows, int SW, long long V, const long
 // Host driver
 // ---------------------------------------------------------------------------
 struct MsWorkspace {
-  DevBuf vis, F0, F1, N, touched, done, rows, q[3], qe[3], tlist, ulist, ctl, srcs, msum;
+  DevBuf vis, F0, F1, N, touched, done, rows, q[3], qe[3], tlist, ulist, ctl, srcs, msum, hq, hqe;
   size_t bytes_rows = 0;
 };
 
@@ -517,7 +565,8 @@ static xbfs_status run_pass(Graph* g, const int32_t* srcs, int n, int* d_out, si
       (st = w.touched.ensure((size_t)(nwords + 64) * 4)) || (st = w.done.ensure((size_t)(nwords + 64) * 4)) ||
       (st = w.rows.ensure((size_t)V * SW * sizeof(RowT))) || (st = w.tlist.ensure((size_t)V * 4 + 4)) ||
       (st = w.ulist.ensure((size_t)(nwords + 64) * 32 * 4)) || (st = w.ctl.ensure(sizeof(ms::Ctl))) ||
-      (st = w.srcs.ensure((size_t)SW * 4)))
+      (st = w.srcs.ensure((size_t)SW * 4)) || (st = w.hq.ensure((size_t)V * 4 + 4)) ||
+      (st = w.hqe.ensure((size_t)V * 4 + 4)))
     return st;
   for (int i = 0; i < 3; ++i)
     if ((st = w.q[i].ensure((size_t)V * 4 + 4)) || (st = w.qe[i].ensure((size_t)V * 4 + 4))) return st;
@@ -540,6 +589,8 @@ static xbfs_status run_pass(Graph* g, const int32_t* srcs, int n, int* d_out, si
   }
   p.tlist = w.tlist.as<int>();
   p.ulist = w.ulist.as<int>();
+  p.hq_ids = w.hq.as<int>();
+  p.hq_eb = w.hqe.as<unsigned>();
   p.ctl = w.ctl.as<ms::Ctl>();
   for (int k = 0; k < W; ++k) {
     const int lo = k * 64, hi = std::min(n, lo + 64);
