@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=32)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the cpu_baseline sample")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the learned / batched / multi-graph / serving comparison sections")
     return ap.parse_args()
 
 
@@ -312,11 +314,158 @@ def run_ours(args):
         "wall_s_timed_region": round(t_wall, 4),
         "hbm_gbs_algorithmic_per_step": round(b_alg * args.steps / (max_ms * 1e-3) / 1e9, 1),
     }
+    if not args.no_extras and args.workload == "rmat":
+        out["learned"] = extra_learned(args, g, srcs, opts, lv, stream, flush, flush_rd, value)
+        g.free()
+        g = None
+        torch.cuda.empty_cache()
+        out["batched"] = extra_batched(args, value)
+        out["multi_graph"] = extra_multigraph(args)
+        out["serve"] = extra_serve(args)
+    if world > 1:
+        # every rank ran the same sections; report the job-wide sums / maxima
+        for key in ("learned", "batched", "multi_graph"):
+            sec = out.get(key)
+            if isinstance(sec, dict) and "gteps" in sec:
+                tot, = allreduce([float(sec["gteps"])], dist.ReduceOp.SUM)
+                sec["gteps_all_ranks"] = round(tot, 3)
     if rank == 0:
         print(json.dumps(out), flush=True)
-    g.free()
+    if g is not None:
+        g.free()
     if world > 1:
         dist.destroy_process_group()
+
+
+def _timed_steps(fn, steps):
+    import torch
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    res = []
+    for i in range(steps):
+        res.append(fn(i, evs[i]))
+    torch.cuda.synchronize()
+    return res, [a.elapsed_time(b) for a, b in evs]
+
+
+def extra_learned(args, g, srcs, opts, lv, stream, flush, flush_rd, plain_gteps):
+    """Same graph and sources with the learned switch (shipped weights)."""
+    from xbfs_b200 import learned
+    path = learned.DEFAULT_WEIGHTS
+    if not os.path.exists(path):
+        return {"unavailable": "no trained weights shipped"}
+    w, meta = learned.load(path)
+    learned.install(w, device=g.device)
+    import dataclasses
+    o2 = dataclasses.replace(opts, policy="mlp")
+    beamer = dataclasses.replace(opts, policy="beamer")
+
+    def run(o):
+        def step(i, ev):
+            flush.fill_(i & 0xFF)
+            flush_rd.sum()
+            ev[0].record(stream)
+            r = g.bfs(int(srcs[i % len(srcs)]), levels=lv, opts=o)
+            ev[1].record(stream)
+            return r
+        res, ms = _timed_steps(step, min(args.steps, 64))
+        return sum(r.edges_mc for r in res) / (sum(ms) * 1e-3) / 1e9
+    g_mlp = run(o2)
+    g_beamer = run(beamer)
+    learned.install(None, device=g.device)
+    return {"gteps": round(g_mlp, 3), "policy": "mlp", "vs_plain": round(g_mlp / plain_gteps, 4),
+            "beamer_gteps": round(g_beamer, 3), "train_meta": {k: meta[k] for k in ("samples", "train_accuracy")}}
+
+
+def extra_batched(args, plain_ref):
+    """512 sources on R-MAT scale 22 ef16 (8 groups of 64 per uint64 word) vs
+    single-source on the same graph; outputs are n x V int32 in HBM."""
+    import torch
+    from xbfs_b200 import Graph, pick_sources
+    g = Graph.rmat(22, 16, args.seed)
+    beg = g.offsets()
+    srcs = pick_sources(beg, 512, args.seed)
+    out = torch.empty((512, g.V), dtype=torch.int32, device="cuda")
+    g.bfs_batch(srcs, levels=out)  # warm-up
+    best = None
+    for _ in range(3):
+        r = g.bfs_batch(srcs, levels=out)
+        if best is None or r.device_ms < best.device_ms:
+            best = r
+    lv = torch.empty(g.V, dtype=torch.int32, device="cuda")
+    ms, mc = 0.0, 0
+    for s in srcs[:64]:
+        r1 = g.bfs(int(s), levels=lv)
+        ms += r1.kernel_ms
+        mc += r1.edges_mc
+    single = mc / (ms * 1e-3) / 1e9
+    res = {"workload": "rmat-s22-ef16, 512 sources", "gteps": round(best.edges_mc / (best.device_ms * 1e-3) / 1e9, 3),
+           "ms": round(best.device_ms, 3), "single_source_gteps_same_graph": round(single, 3)}
+    res["vs_single_source"] = round(res["gteps"] / single, 3)
+    del out
+    g.free()
+    torch.cuda.empty_cache()
+    return res
+
+
+def extra_multigraph(args):
+    """256 uneven graphs (128 R-MAT scale 10..18 ef 8..32 + 128 ER n 1e3..2e5,
+    mean degree 8), one source each, one persistent launch replayed from a
+    CUDA graph, configuration picked by the autotuner; vs one xbfs_bfs call
+    per graph."""
+    import torch
+    from xbfs_b200 import Graph, MultiGraph, pick_sources
+    rng = np.random.default_rng(args.seed)
+    graphs = [Graph.rmat(int(rng.integers(10, 19)), int(rng.integers(8, 33)), 100 + i) for i in range(128)]
+    graphs += [Graph.er(int(rng.integers(1000, 200001)), 8.0, 300 + i) for i in range(128)]
+    srcs = np.array([int(pick_sources(g.offsets(), 1, 7 + i)[0]) for i, g in enumerate(graphs)], dtype=np.int32)
+    mg = MultiGraph(graphs)
+    cfg = mg.tune(srcs, reps=2)
+    out = torch.empty(mg.total_V, dtype=torch.int32, device="cuda")
+    best = min((mg.bfs(srcs, levels=out) for _ in range(5)), key=lambda r: r.device_ms)
+    t_one, mc1 = 0.0, 0
+    for g, s in zip(graphs, srcs):
+        r = g.bfs(int(s))
+        t_one += r.device_ms
+        mc1 += r.edges_mc
+    res = {"workload": "256 graphs (128 R-MAT s10-18, 128 ER 1e3-2e5)", "gteps": round(best.edges_mc / (best.device_ms * 1e-3) / 1e9, 3),
+           "ms": round(best.device_ms, 3), "tuned": cfg, "one_call_per_graph_ms": round(t_one, 3),
+           "speedup_vs_one_call_per_graph": round(t_one / best.device_ms, 2)}
+    mg.free()
+    for g in graphs:
+        g.free()
+    del out
+    torch.cuda.empty_cache()
+    return res
+
+
+def extra_serve(args):
+    """Serving: Poisson arrivals over 8 device-resident graphs (R-MAT scales
+    20-24 ef16 and grids 2048x2048, 4096x4096, 8192x2048), continuous batching
+    into 64-source slots, admission by free HBM; p50 / p99 latency and
+    aggregate GTEPS per arrival rate."""
+    import torch
+    from xbfs_b200 import Graph, pick_sources
+    from xbfs_b200.api import Server
+    specs = [("rmat", s) for s in (20, 21, 22, 23, 24)] + [("grid", 2048, 2048), ("grid", 4096, 4096), ("grid", 8192, 2048)]
+    graphs = [Graph.rmat(sp[1], 16, args.seed + sp[1]) if sp[0] == "rmat" else Graph.grid(sp[1], sp[2]) for sp in specs]
+    begs = [g.offsets() for g in graphs]
+    srv = Server(graphs)
+    res = {"graphs": ["rmat-s%d-ef16" % sp[1] if sp[0] == "rmat" else "grid-%dx%d" % sp[1:] for sp in specs], "rates": []}
+    rng = np.random.default_rng(args.seed)
+    for rate in (1e2, 1e3, 1e4, 1e5):
+        n = int(min(400, max(40, rate * 2)))
+        gid = rng.integers(0, len(graphs), size=n).astype(np.int32)
+        src = np.array([pick_sources(begs[gi], 1, int(rate) + i)[0] for i, gi in enumerate(gid)], dtype=np.int32)
+        arr = np.cumsum(rng.exponential(1e6 / rate, size=n))
+        r = srv.run(gid, src, arr, keep_outputs=False)
+        res["rates"].append({"rate_per_s": rate, "requests": n, "p50_ms": round(r["p50_us"] / 1e3, 3),
+                             "p99_ms": round(r["p99_us"] / 1e3, 3), "gteps": round(r["gteps"], 3),
+                             "wall_s": round(r["wall_us"] / 1e6, 3)})
+    srv.free()
+    for g in graphs:
+        g.free()
+    torch.cuda.empty_cache()
+    return res
 
 
 def run_reference(args):

@@ -182,6 +182,27 @@ xbfs_status xbfs_multi_tune(xbfs_multi* m, const int32_t* srcs, int32_t reps, in
 xbfs_status xbfs_multi_set_config(xbfs_multi* m, int32_t block, int32_t thread_max, float alpha);
 void xbfs_multi_free(xbfs_multi* m);
 
+/* Serving loop (no reference counterpart): BFS requests over device-resident
+ * graphs, continuously batched 64 per graph into uint64 bit slots; a request
+ * joins a running batch at any level step, is admitted when a slot is free
+ * and its int32[V] output fits the HBM budget (hbm_budget_bytes <= 0: free
+ * memory minus 2 GiB), and leaves when its traversal is complete. */
+typedef struct xbfs_server xbfs_server;
+xbfs_status xbfs_serve_create(xbfs_graph* const* graphs, int32_t n, int32_t device, int64_t hbm_budget_bytes,
+                              xbfs_server** out);
+/* Replays a request trace in real time (request i targets graph[i] from
+ * src[i] and arrives arrival_us[i] after the start). Returns per request the
+ * admission and completion times (us since start) and its Graph500 edge
+ * count; with keep_outputs, levels[i] = device pointer to its level array
+ * (free with xbfs_serve_release). */
+xbfs_status xbfs_serve_run(xbfs_server* s, int32_t n, const int32_t* graph, const int32_t* src,
+                           const double* arrival_us, int32_t keep_outputs, double* admit_us, double* finish_us,
+                           int64_t* edges_mc, int32_t** levels, double* wall_us);
+xbfs_status xbfs_serve_release(xbfs_server* s, int32_t* levels_dev, int64_t V);
+/* Copies a kept level array (V entries) to host memory, then releases it. */
+xbfs_status xbfs_serve_fetch(xbfs_server* s, int32_t* levels_dev, int64_t V, int32_t* host_out);
+void xbfs_serve_free(xbfs_server* s);
+
 /* Per-level trace of the last xbfs_bfs call made with opts.trace = 1
  * (replaces the reference's tag[]/ratio[]/iter[] arrays, written to
  * Hybrid_iteration.csv at bfs_gpu_update.cu:270-272). */
@@ -233,6 +254,15 @@ xbfs_status xbfs_gen_grid_host(int32_t width, int32_t height, int64_t** beg, int
 xbfs_status xbfs_gen_er_host(int64_t n, double mean_degree, uint64_t seed, int64_t** beg,
                              int32_t** csr, int64_t* V, int64_t* E);
 void xbfs_free_host(void* p);
+/* Edge-list text (one "u v" pair per line, '#'/'%' comments, skip_lines
+ * header lines) -> <out_prefix>_beg_pos.bin + <out_prefix>_csr.bin (int32
+ * neighbours). Replaces CSRGenerator/tuple_text_to_bin.cpp (:59-426), which
+ * writes int64 neighbours its own reader cannot load. reverse = 1 adds every
+ * tuple's reversed edge; dedupe / drop_self_loops as named; write_weights
+ * adds <out_prefix>_weight.bin (int32, 1..63, seeded), which the BFS ignores. */
+xbfs_status xbfs_convert_edge_list(const char* text_path, int32_t reverse, int32_t skip_lines, int32_t dedupe,
+                                   int32_t drop_self_loops, int32_t write_weights, const char* out_prefix,
+                                   int64_t* V, int64_t* E);
 /* Deterministic source sampling: k sources uniform over vertices with
  * degree > 0 (host CSR offsets). */
 xbfs_status xbfs_pick_sources(const int64_t* beg, int64_t V, int32_t k, uint64_t seed,

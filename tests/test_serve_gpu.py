@@ -1,0 +1,68 @@
+"""Serving loop: requests arriving while others run join the 64-slot batches
+of their graph; every result must equal the same request run alone
+(xbfs_bfs) and the CPU oracle, whatever the arrival pattern, slot pressure
+or HBM budget. Latencies are reported."""
+import numpy as np
+import pytest
+
+import oracle
+from xbfs_b200 import Graph, gen_er_host, gen_grid_host, gen_rmat_host, pick_sources
+from xbfs_b200.api import Server
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(seed=0):
+    cpu = [gen_rmat_host(12, 16, 40 + seed), gen_rmat_host(14, 8, 41 + seed), gen_er_host(20000, 8.0, 42 + seed),
+           gen_grid_host(64, 48)]
+    graphs = [Graph.from_csr(b, c) for b, c in cpu]
+    return cpu, graphs
+
+
+def trace(cpu, n, rate_per_s, seed):
+    rng = np.random.default_rng(seed)
+    gid = rng.integers(0, len(cpu), size=n).astype(np.int32)
+    src = np.array([pick_sources(cpu[g][0], 1, int(seed * 1000 + i))[0] for i, g in enumerate(gid)], dtype=np.int32)
+    arr = np.cumsum(rng.exponential(1e6 / rate_per_s, size=n))
+    return gid, src, arr
+
+
+def check_all(srv, cpu, graphs, gid, src, res):
+    for i, (g, s) in enumerate(zip(gid, src)):
+        V = graphs[g].V
+        lv = srv.fetch(res["levels_dev"][i], V)
+        alone = graphs[g].bfs(int(s)).levels
+        ref = oracle.bfs_queue(cpu[g][0], cpu[g][1], int(s))
+        assert np.array_equal(lv, ref), f"request {i} (graph {g}, source {s}) differs in the mix"
+        assert np.array_equal(alone, ref)
+        assert res["edges_mc"][i] == oracle.edges_mc(cpu[g][0], ref)
+
+
+@pytest.mark.parametrize("rate", [2e3, 5e4, 1e7])
+def test_results_in_the_mix_equal_results_alone(rate):
+    cpu, graphs = setup(0)
+    gid, src, arr = trace(cpu, 150, rate, 1)
+    srv = Server(graphs)
+    res = srv.run(gid, src, arr, keep_outputs=True)
+    assert np.all(res["finish_us"] >= res["admit_us"]) and np.all(res["admit_us"] >= arr - 1)
+    print(f"rate {rate:g}/s: p50 {res['p50_us']:.0f} us, p99 {res['p99_us']:.0f} us, {res['gteps']:.2f} GTEPS")
+    check_all(srv, cpu, graphs, gid, src, res)
+
+
+def test_more_requests_than_slots_and_a_tight_memory_budget():
+    cpu, graphs = setup(1)
+    gid, src, arr = trace(cpu, 300, 1e8, 2)   # everything arrives at once: > 64 per graph
+    budget = 3 * max(g.V for g in graphs) * 4   # room for three outputs at a time
+    srv = Server(graphs, hbm_budget_bytes=budget)
+    res = srv.run(gid, src, arr, keep_outputs=True)
+    check_all(srv, cpu, graphs, gid, src, res)
+
+
+def test_run_without_keeping_outputs_reports_edges():
+    cpu, graphs = setup(2)
+    gid, src, arr = trace(cpu, 100, 1e5, 3)
+    srv = Server(graphs)
+    res = srv.run(gid, src, arr, keep_outputs=False)
+    for i, (g, s) in enumerate(zip(gid, src)):
+        assert res["edges_mc"][i] == oracle.edges_mc(cpu[g][0], oracle.bfs_queue(cpu[g][0], cpu[g][1], int(s)))
+    assert res["p99_us"] >= res["p50_us"] > 0

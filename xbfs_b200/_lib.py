@@ -126,6 +126,7 @@ SIGNATURES = {
     "xbfs_gen_grid_host": (_i32, [_i32, _i32, _PPI64, _PPI32, _PI64, _PI64]),
     "xbfs_gen_er_host": (_i32, [_i64, _f64, _u64, _PPI64, _PPI32, _PI64, _PI64]),
     "xbfs_free_host": (None, [_p]),
+    "xbfs_convert_edge_list": (_i32, [C.c_char_p, _i32, _i32, _i32, _i32, _i32, C.c_char_p, _PI64, _PI64]),
     "xbfs_pick_sources": (_i32, [_p, _i64, _i32, _u64, _p]),
     "xbfs_bfs_batch": (_i32, [_p, _p, _i32, _p, C.POINTER(Opts), C.POINTER(Stats)]),
     "xbfs_bfs_batch_w": (_i32, [_p, _p, _i32, _p, C.POINTER(Opts), C.POINTER(Stats), _i32]),
@@ -136,6 +137,11 @@ SIGNATURES = {
     "xbfs_multi_set_config": (_i32, [_p, _i32, _i32, _f32]),
     "xbfs_multi_free": (None, [_p]),
     "xbfs_level_costs": (_i32, [_p, _i32, _i32, _i32, _p, C.POINTER(LevelTrace), _PI32]),
+    "xbfs_serve_create": (_i32, [C.POINTER(_p), _i32, _i32, _i64, C.POINTER(_p)]),
+    "xbfs_serve_run": (_i32, [_p, _i32, _p, _p, _p, _i32, _p, _p, _p, _p, C.POINTER(C.c_double)]),
+    "xbfs_serve_release": (_i32, [_p, _p, _i64]),
+    "xbfs_serve_fetch": (_i32, [_p, _p, _i64, _p]),
+    "xbfs_serve_free": (None, [_p]),
     "xbfs_mlp_num_params": (_i32, []),
     "xbfs_mlp_set_weights": (_i32, [_i32, _p, _i32]),
     "xbfs_mlp_logits": (_i32, [_i32, _p, _p, _i32, _p]),

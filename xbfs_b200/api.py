@@ -280,6 +280,15 @@ def pick_sources(beg: np.ndarray, k: int, seed: int = 1) -> np.ndarray:
     return out[:k]
 
 
+def convert_edge_list(text_path: str, out_prefix: str, reverse: bool = True, skip_lines: int = 0,
+                      dedupe: bool = True, drop_self_loops: bool = True, weights: bool = False) -> tuple[int, int]:
+    """Edge-list text -> CSR file pair (int64 offsets, int32 neighbours)."""
+    V, E = C.c_int64(), C.c_int64()
+    check(lib.xbfs_convert_edge_list(text_path.encode(), int(reverse), int(skip_lines), int(dedupe),
+                                     int(drop_self_loops), int(weights), out_prefix.encode(), C.byref(V), C.byref(E)))
+    return V.value, E.value
+
+
 def write_csr(beg: np.ndarray, csr: np.ndarray, beg_path: str, csr_path: str) -> None:
     """Write the reference's file pair: raw int64 beg_pos, raw int32 csr."""
     np.ascontiguousarray(beg, dtype="<i8").tofile(beg_path)
@@ -334,6 +343,56 @@ class MultiGraph:
     def free(self) -> None:
         if self._h:
             lib.xbfs_multi_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching BFS server over device-resident graphs (xbfs_serve_*)."""
+
+    def __init__(self, graphs: Sequence[Graph], device: int = 0, hbm_budget_bytes: int = 0):
+        arr = (C.c_void_p * len(graphs))(*[g.handle.value for g in graphs])
+        h = C.c_void_p()
+        check(lib.xbfs_serve_create(arr, len(graphs), device, int(hbm_budget_bytes), C.byref(h)))
+        self._h = h
+        self.graphs = list(graphs)
+
+    def run(self, graph_ids, srcs, arrival_us, keep_outputs: bool = False) -> dict:
+        g = np.ascontiguousarray(graph_ids, dtype=np.int32)
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        a = np.ascontiguousarray(arrival_us, dtype=np.float64)
+        n = len(g)
+        admit = np.zeros(n, dtype=np.float64)
+        fin = np.zeros(n, dtype=np.float64)
+        mc = np.zeros(n, dtype=np.int64)
+        ptrs = (C.c_void_p * max(n, 1))()
+        wall = C.c_double(0)
+        check(lib.xbfs_serve_run(self._h, n, g.ctypes.data, s.ctypes.data, a.ctypes.data, 1 if keep_outputs else 0,
+                                 admit.ctypes.data, fin.ctypes.data, mc.ctypes.data,
+                                 C.cast(ptrs, C.c_void_p) if keep_outputs else None, C.byref(wall)))
+        lat = fin - a
+        out = {"admit_us": admit, "finish_us": fin, "latency_us": lat, "edges_mc": mc, "wall_us": wall.value,
+               "p50_us": float(np.percentile(lat, 50)) if n else 0.0,
+               "p99_us": float(np.percentile(lat, 99)) if n else 0.0,
+               "gteps": float(mc.sum() / (wall.value * 1e-6) / 1e9) if wall.value > 0 else 0.0}
+        if keep_outputs:
+            out["levels_dev"] = [ptrs[i] for i in range(n)]
+        return out
+
+    def fetch(self, ptr: int, V: int) -> np.ndarray:
+        """Copy one kept device level array to the host and release it."""
+        host = np.empty(V, dtype=np.int32)
+        check(lib.xbfs_serve_fetch(self._h, C.c_void_p(ptr), V, host.ctypes.data))
+        return host
+
+    def free(self) -> None:
+        if self._h:
+            lib.xbfs_serve_free(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

@@ -92,13 +92,14 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False, p
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
-    cli_src = os.path.join(CSRC, "bfs_cli.cpp")
-    if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB] + heads)):
-        cmd = ["g++", "-O2", "-std=c++17", "-I" + INCLUDE, cli_src, "-o", CLI,
-               "-L" + PKG, "-lxbfs", "-Wl,-rpath,$ORIGIN/.."]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError("bfs CLI link failed:\n" + r.stdout + r.stderr)
+    for cli_name, exe in (("bfs_cli.cpp", CLI), ("text_to_bin_cli.cpp", os.path.join(PKG, "bin", "text_to_bin"))):
+        cli_src = os.path.join(CSRC, cli_name)
+        if os.path.exists(cli_src) and (force or _stale(exe, [cli_src, LIB] + heads)):
+            cmd = ["g++", "-O2", "-std=c++17", "-I" + INCLUDE, cli_src, "-o", exe,
+                   "-L" + PKG, "-lxbfs", "-Wl,-rpath,$ORIGIN/.."]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"{cli_name} link failed:\n" + r.stdout + r.stderr)
     return LIB
 
 

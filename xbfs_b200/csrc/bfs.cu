@@ -38,12 +38,11 @@
 //  * A top-down level whose frontier is only in bitmap form (after bottom-up
 //    or single-scan) compacts and expands the bitmap in the same phase
 //    ("single scan"), CTA by CTA, instead of building a queue first.
-//  * Bottom-up: every warp takes 1024-vertex chunks from a global counter,
-//    compacts the chunk's unvisited vertices with a warp popcount scan (the
-//    reference's ballot_counting + prefix sum + FQ_gen, without the host round
-//    trip of my_prefixsum) and lanes probe eight neighbours at a time with
-//    early exit and the reference's asynchronous level+2 rule; no CTA-wide
-//    synchronisation until the level ends.
+//  * Bottom-up: every CTA compacts the unvisited vertices of its slice with
+//    block ballot/popcount scans (the reference's ballot_counting + prefix
+//    sum + FQ_gen, without the host round trip of my_prefixsum); its warps
+//    drain the list dynamically and lanes probe 2, 4, then 8 neighbours at a
+//    time with early exit and the reference's asynchronous level+2 rule.
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -67,7 +66,6 @@ constexpr int kCapL = 256;          // staging capacity, large bin
 constexpr int kFlushAt = kCap - kTE;
 constexpr int kFlushAtL = kCapL / 2;  // large-bin overflow goes straight to the global queue
 constexpr int kTileW = kWin / 32;   // bitmap words per dense fused-sweep sub-tile
-constexpr int kBuChunkW = 32;       // bitmap words per bottom-up warp chunk (1024 vertices)
 constexpr int kHeavyDeg = 4096;     // fused sweep: larger degrees are deferred to the heavy list
 
 constexpr unsigned long long kCountMask = (1ull << 31) - 1;
@@ -96,7 +94,6 @@ struct Ctl {
   unsigned long long reached;   // sum of frontier sizes
   unsigned long long msum;      // sum of frontier degrees
   unsigned long long heavy[2];  // packed counter of the heavy list, by level parity
-  unsigned int bu_chunk[2];     // bottom-up chunk dispenser, by level parity
   int strat_count[4];
   FDesc fd[4];
 };
@@ -117,6 +114,7 @@ struct Params {
   uint32_t* fb[4];
   QBin q[2][3];
   QBin heavy;
+  int* ulist;        // bottom-up lists, one region per CTA slice
   Ctl* ctl;
   LevelRecDev* hist;
   int hist_cap;
@@ -622,89 +620,76 @@ __device__ __forceinline__ void probe_range(const Params& p, const uint32_t* fbc
   }
 }
 
-// Bottom-up step for level L. CTAs take 2048-vertex chunks from a global
-// dispenser, compact the unvisited vertices of a chunk (sorted) into shared
-// memory and let each lane search one vertex's neighbours, eight at a time.
+// Bottom-up step for level L. Each CTA owns a contiguous slice of the vertex
+// range (vertex ids are scrambled, so slices carry similar work): it compacts
+// the slice's unvisited vertices into a sorted list with block ballot /
+// popcount scans (the reference's ballot_counting + prefix sum + FQ_gen,
+// without the host round trip of my_prefixsum), then its warps drain the list
+// 32 vertices at a time from a shared counter, so a slow warp does not hold the
+// others. Each lane probes its vertex's neighbours 2, then 4, then 8 at a time
+// (most vertices find a parent among the first few).
 template <bool PAR, bool ASYNC>
 __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
                           uint32_t* fbn2) {
   const long long nw = p.nwords;
-  const long long nchunks = (nw + kBuChunkW - 1) / kBuChunkW;
-  unsigned* disp = &p.ctl->bu_chunk[L & 1];
+  const long long G = gridDim.x, b = blockIdx.x;
+  const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
+  int* list = p.ulist + w0 * 32;
+  long long pos = 0;
+  for (long long wb = w0; wb < w1; wb += kBlock) {
+    const long long w = wb + threadIdx.x;
+    uint32_t bits = (w < w1) ? ~ld_cg_u32(p.vis + w) : 0u;
+    long long total;
+    const long long ex = block_exclusive_scan<kBlock, long long>((long long)__popc(bits), sm.red, &total);
+    long long o = pos + ex;
+    while (bits) {
+      const int bp = __ffs(bits) - 1;
+      bits &= bits - 1;
+      list[o++] = (int)(w * 32 + bp);
+    }
+    pos += total;
+  }
+  if (threadIdx.x == 0) sm.bu_next = 0;
+  __syncthreads();
+  const int n = (int)pos;
   const int lane = threadIdx.x & 31;
-  // Each warp works alone: it takes a 1024-vertex chunk from the dispenser,
-  // compacts the chunk's unvisited vertices (lane = bitmap word, warp scan of
-  // the popcounts) into its own shared list, and drains it 32 at a time. The
-  // lists alias the top-down staging area, which is idle during bottom-up.
-  static_assert(sizeof(int) * 2 * kCap * 2 + sizeof(long long) * 2 * kCap >=
-                    sizeof(int) * (kBlock / 32) * kBuChunkW * 32,
-                "bottom-up lists must fit in the staging area");
-  int* list = reinterpret_cast<int*>(&sm.st_id[0][0]) + (threadIdx.x >> 5) * (kBuChunkW * 32);
   for (;;) {
-    unsigned c = 0;
-    if (lane == 0) c = atomicAdd(disp, 1u);
-    c = __shfl_sync(0xffffffffu, c, 0);
-    if ((long long)c >= nchunks) break;
-    const long long w = (long long)c * kBuChunkW + lane;
-    uint32_t bits = (w < nw) ? ~ld_cg_u32(p.vis + w) : 0u;
-    const int cb = __popc(bits);
-    const int incl = warp_inclusive_scan(cb);
-    const int n = __shfl_sync(0xffffffffu, incl, 31);
-    {
-      int o = incl - cb;
-      while (bits) {
-        const int bp = __ffs(bits) - 1;
-        bits &= bits - 1;
-        list[o++] = (int)(w * 32 + bp);
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&sm.bu_next, 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const int i = base + lane;
+    if (i < n) {
+      const int v = list[i];
+      const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
+      int found = -1, found2 = -1;
+      long long e = e0;
+      if (p.bu_mode == 1) {  // streaming (L1-bypassing) neighbour loads
+        probe_range<2, false, ASYNC>(p, fbc, fbn, e, e0 + 2 < e1 ? e0 + 2 : e1, found, found2);
+        if (found < 0) probe_range<4, false, ASYNC>(p, fbc, fbn, e, e0 + 6 < e1 ? e0 + 6 : e1, found, found2);
+        if (found < 0) probe_range<8, false, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+      } else {  // L1-allocating neighbour loads: the next probes hit the same sector
+        probe_range<2, true, ASYNC>(p, fbc, fbn, e, e0 + 2 < e1 ? e0 + 2 : e1, found, found2);
+        if (found < 0) probe_range<4, true, ASYNC>(p, fbc, fbn, e, e0 + 6 < e1 ? e0 + 6 : e1, found, found2);
+        if (found < 0) probe_range<8, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+      }
+      const uint32_t word = (uint32_t)v >> 5, bit = 1u << (v & 31);
+      if (found >= 0) {
+        p.levels[v] = L + 1;
+        if (PAR) p.parents[v] = found;
+        red_or_u32(p.vis + word, bit);
+        red_or_u32(fbn + word, bit);
+        acc.n1 += 1;
+        acc.m1 += e1 - e0;
+      } else if (ASYNC && found2 >= 0) {
+        p.levels[v] = L + 2;
+        if (PAR) p.parents[v] = found2;
+        red_or_u32(p.vis + word, bit);
+        red_or_u32(fbn2 + word, bit);
+        acc.n2 += 1;
+        acc.m2 += e1 - e0;
       }
     }
-    __syncwarp();
-    for (int base = 0; base < n; base += 32) {
-      const int i = base + lane;
-      if (i < n) {
-        const int v = list[i];
-        const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
-        int found = -1, found2 = -1;
-        long long e = e0;
-        switch (p.bu_mode) {
-          case 1:  // 4 at a time, streaming loads
-            probe_range<4, false, ASYNC>(p, fbc, fbn, e, e1, found, found2);
-            break;
-          case 2:  // 8 at a time, L1-allocating loads
-            probe_range<8, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
-            break;
-          case 3:  // 4 at a time, L1-allocating loads
-            probe_range<4, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
-            break;
-          case 4:  // widening 2 / 4 / 8, L1-allocating loads
-            probe_range<2, true, ASYNC>(p, fbc, fbn, e, e0 + 2 < e1 ? e0 + 2 : e1, found, found2);
-            if (found < 0) probe_range<4, true, ASYNC>(p, fbc, fbn, e, e0 + 6 < e1 ? e0 + 6 : e1, found, found2);
-            if (found < 0) probe_range<8, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
-            break;
-          default:  // widening 2 / 4 / 8, streaming loads
-            probe_range<2, false, ASYNC>(p, fbc, fbn, e, e0 + 2 < e1 ? e0 + 2 : e1, found, found2);
-            if (found < 0) probe_range<4, false, ASYNC>(p, fbc, fbn, e, e0 + 6 < e1 ? e0 + 6 : e1, found, found2);
-            if (found < 0) probe_range<8, false, ASYNC>(p, fbc, fbn, e, e1, found, found2);
-        }
-        const uint32_t word = (uint32_t)v >> 5, bit = 1u << (v & 31);
-        if (found >= 0) {
-          p.levels[v] = L + 1;
-          if (PAR) p.parents[v] = found;
-          red_or_u32(p.vis + word, bit);
-          red_or_u32(fbn + word, bit);
-          acc.n1 += 1;
-          acc.m1 += e1 - e0;
-        } else if (ASYNC && found2 >= 0) {
-          p.levels[v] = L + 2;
-          if (PAR) p.parents[v] = found2;
-          red_or_u32(p.vis + word, bit);
-          red_or_u32(fbn2 + word, bit);
-          acc.n2 += 1;
-          acc.m2 += e1 - e0;
-        }
-      }
-    }
-    __syncwarp();
   }
 }
 
@@ -881,9 +866,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       if (blockIdx.x == 0) {
         if (L < p.hist_cap) p.hist[L].strategy = S;
         st_strat[S] += 1;
-        // counters used at level L+1 (last used at level L-1)
+        // counter used at level L+1 (last used at level L-1)
         ctl->heavy[(L + 1) & 1] = 0ull;
-        ctl->bu_chunk[(L + 1) & 1] = 0u;
       }
     }
     // ---- housekeeping for slots no longer in use (first phase of the level)
@@ -993,6 +977,7 @@ static xbfs_status ensure_workspace(Graph* g, int small_max, int medium_max) {
     if ((st = w.bits.ensure((size_t)nwords * 4 * 5))) return st;
     if ((st = w.ctl.ensure(sizeof(Ctl)))) return st;
     if ((st = w.rs.ensure(sizeof(ResumeState)))) return st;
+    if ((st = w.ulist.ensure((size_t)nwords * 32 * 4))) return st;
     w.hist_cap = 1 << 16;
     if ((st = w.hist.ensure(sizeof(LevelRecDev) * (size_t)w.hist_cap))) return st;
     // heavy list of the fused sweep: vertices with degree > kHeavyDeg (<= degree > 16)
@@ -1052,6 +1037,7 @@ static xbfs_status setup_params(Graph* g, const xbfs_opts& o, int* d_levels, int
   p.heavy.ids = w.heavy_ids.as<int>();
   p.heavy.eb = w.heavy_eb.as<unsigned>();
   p.heavy.bg = w.heavy_bg.as<long long>();
+  p.ulist = w.ulist.as<int>();
   p.ctl = w.ctl.as<Ctl>();
   p.hist = w.hist.as<LevelRecDev>();
   p.hist_cap = w.hist_cap;

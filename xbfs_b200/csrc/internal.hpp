@@ -55,6 +55,7 @@ struct SsWorkspace {
   DevBuf qbg[2][3];        // per parity, per bin: CSR offsets (int64)
   size_t qcap[3] = {0, 0, 0};
   DevBuf heavy_ids, heavy_eb, heavy_bg;  // heavy vertices deferred by a fused sweep
+  DevBuf ulist;            // bottom-up lists of unvisited vertices
   DevBuf ctl;              // control block
   DevBuf rs;               // loop state of a stepped traversal
   DevBuf snap;             // snapshot of the whole traversal state (stepped mode)

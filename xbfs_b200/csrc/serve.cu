@@ -1,0 +1,578 @@
+// Serving loop: BFS requests over device-resident graphs, continuously
+// batched into 64-source bit slots.
+//
+// No counterpart in the reference. Design:
+//  * Each graph owns a slot batch: one uint64 word per vertex for visited,
+//    frontier (two, by tick parity) and an accumulator; bit s belongs to
+//    slot s. A request joins a running batch at any tick t: its bit is set at
+//    its source and its join tick recorded; from then on every tick advances
+//    all slots by one level, and a vertex that gains bit s at tick t gets
+//    level t + 1 - join[s] in that request's own int32[V] output.
+//  * A slot finishes at the first tick that gives it no new vertex; its
+//    visited bits are cleared and the slot is reused. Requests wait for a
+//    free slot and for room in an HBM budget (their output array is
+//    allocated from a stream-ordered pool when admitted).
+//  * Ticks are top-down: the frontier queue (vertex ids with exclusive edge
+//    offsets) is expanded edge-balanced across the GPU, touched vertices are
+//    merged, their new bits recorded and queued for the next tick. Graphs run
+//    on their own streams so their ticks overlap on the device; the host
+//    intervenes every K ticks (K grows with a graph's observed depth, so
+//    long-diameter graphs are not host-bound).
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <deque>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace xbfs {
+namespace sv {
+
+constexpr int kBlock = 512;
+constexpr int kSlots = 64;
+constexpr int kRing = 64;  // ticks between host interventions, at most
+constexpr unsigned long long kCountMask = (1ull << 31) - 1;
+
+struct Ctl {
+  unsigned long long q[3];            // packed (edges << 31) | count, frontier queue ring
+  unsigned int tcount[2];             // touched-list length by tick parity
+  unsigned long long active[kRing];   // OR of the bits gained at each tick of the window
+  unsigned long long msum[kSlots];    // per slot: sum of degrees of reached vertices
+};
+
+struct Params {
+  const long long* beg;
+  const int* csr;
+  long long V;
+  unsigned long long* vis;
+  unsigned long long* F[2];
+  unsigned long long* N;
+  uint32_t* touched;
+  int* tlist;
+  int* qids[3];
+  unsigned* qeb[3];
+  int* const* out;     // device table: output array of each slot (or null)
+  const long long* join;  // device table: join tick of each slot
+  Ctl* ctl;
+};
+
+// tick t reads frontier F[t&1] and queue t%3, writes F[(t+1)&1] and queue (t+1)%3
+__global__ void __launch_bounds__(kBlock) k_sv_expand(Params p, long long t) {
+  __shared__ long long wbeg[kBlock + 1];
+  __shared__ unsigned web[kBlock + 1];
+  __shared__ int wu[kBlock + 1];
+  __shared__ int next_s;
+  const int lane = threadIdx.x & 31;
+  const int qs = (int)(t % 3);
+  const unsigned long long pk = ld_cg_u64(&p.ctl->q[qs]);
+  const unsigned cnt = (unsigned)(pk & kCountMask);
+  const unsigned long long M = pk >> 31;
+  const unsigned long long G = gridDim.x;
+  const unsigned long long lo = M * blockIdx.x / G, hi = M * (blockIdx.x + 1) / G;
+  if (cnt == 0 || lo >= hi) return;
+  const int* ids = p.qids[qs];
+  const unsigned* eb = p.qeb[qs];
+  const unsigned long long* Fc = p.F[t & 1];
+  unsigned* tctr = &p.ctl->tcount[t & 1];
+  if (threadIdx.x < 32) {
+    unsigned a = 0, b = cnt;
+    while (b - a > 32) {
+      const unsigned span = b - a;
+      const unsigned piv = a + (unsigned)(((unsigned long long)span * lane) / 32);
+      const unsigned m = __ballot_sync(0xffffffffu, (unsigned long long)eb[piv] <= lo);
+      const int last = 31 - __clz(m);
+      const unsigned na = a + (unsigned)(((unsigned long long)span * last) / 32);
+      const unsigned nb = (last == 31) ? b : a + (unsigned)(((unsigned long long)span * (last + 1)) / 32);
+      a = na;
+      b = nb;
+    }
+    const unsigned idx = a + lane;
+    const unsigned m = __ballot_sync(0xffffffffu, idx < b && (unsigned long long)eb[idx] <= lo);
+    if (lane == 0) next_s = (int)(a + 31 - __clz(m));
+  }
+  __syncthreads();
+  unsigned s = (unsigned)next_s;
+  for (unsigned long long r = lo; r < hi; r += kBlock) {
+    const unsigned long long rhi = (r + kBlock < hi) ? r + kBlock : hi;
+    for (int i = threadIdx.x; i <= kBlock; i += kBlock) {
+      const unsigned slot = s + (unsigned)i;
+      unsigned e0 = 0xffffffffu;
+      if (slot < cnt) {
+        const unsigned x = eb[slot];
+        if ((unsigned long long)x < rhi) {
+          e0 = x;
+          const int u = ids[slot];
+          wu[i] = u;
+          wbeg[i] = ld_nc_i64(p.beg + u);
+        }
+      }
+      web[i] = e0;
+    }
+    __syncthreads();
+    const unsigned long long e = r + threadIdx.x;
+    bool first = false;
+    int v = 0;
+    if (e < rhi) {
+      int a = 0, c = kBlock + 1;
+      while (c - a > 1) {
+        const int mid = (a + c) >> 1;
+        if ((unsigned long long)web[mid] <= e) a = mid; else c = mid;
+      }
+      const int u = wu[a];
+      v = ld_stream_i32(p.csr + wbeg[a] + (long long)(e - web[a]));
+      const unsigned long long m = Fc[u] & ~ld_cg_u64(p.vis + v);
+      if (m) {
+        red_or_u64(p.N + v, m);
+        const uint32_t bit = 1u << (v & 31);
+        if (!(ld_cg_u32(p.touched + (v >> 5)) & bit)) first = !(atomicOr(p.touched + (v >> 5), bit) & bit);
+      }
+    }
+    const unsigned tm = __ballot_sync(0xffffffffu, first);
+    if (tm) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(tctr, (unsigned)__popc(tm));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (first) p.tlist[base + __popc(tm & ((1u << lane) - 1))] = v;
+    }
+    if (threadIdx.x == 0 && rhi < hi) {
+      int a = 0, c = kBlock + 1;
+      while (c - a > 1) {
+        const int mid = (a + c) >> 1;
+        if ((unsigned long long)web[mid] <= rhi) a = mid; else c = mid;
+      }
+      next_s = (int)(s + a);
+    }
+    __syncthreads();
+    s = (unsigned)next_s;
+  }
+}
+
+// Merge the touched vertices of tick t: new bits become visited and the next
+// frontier, each new (vertex, slot) gets its level in the slot's output, the
+// vertex is queued for tick t+1, and the tick's gained-bit mask is recorded.
+__global__ void __launch_bounds__(kBlock) k_sv_merge(Params p, long long t) {
+  __shared__ unsigned long long s_msum[kSlots];
+  __shared__ unsigned long long s_act;
+  if (threadIdx.x < kSlots) s_msum[threadIdx.x] = 0;
+  if (threadIdx.x == 0) s_act = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned tc = ld_cg_u32(&p.ctl->tcount[t & 1]);
+  const int qn = (int)((t + 1) % 3);
+  unsigned long long* Fn = p.F[(t + 1) & 1];
+  unsigned long long act = 0;
+  for (long long i0 = blockIdx.x * (long long)kBlock; i0 < tc; i0 += (long long)gridDim.x * kBlock) {
+    const long long i = i0 + threadIdx.x;
+    bool have = false;
+    int v = 0;
+    long long deg = 0;
+    if (i < tc) {
+      v = p.tlist[i];
+      p.touched[v >> 5] = 0u;
+      const unsigned long long a = p.N[v];
+      p.N[v] = 0ull;
+      const unsigned long long vv = p.vis[v];
+      const unsigned long long nw = a & ~vv;
+      if (nw) {
+        p.vis[v] = vv | nw;
+        Fn[v] = nw;
+        act |= nw;
+        const long long b0 = ld_nc_i64(p.beg + v);
+        deg = ld_nc_i64(p.beg + v + 1) - b0;
+        unsigned long long bits = nw;
+        while (bits) {
+          const int s = __ffsll((long long)bits) - 1;
+          bits &= bits - 1;
+          int* o = p.out[s];
+          if (o) o[v] = (int)(t + 1 - p.join[s]);
+          if (deg) atomicAdd(&s_msum[s], (unsigned long long)deg);
+        }
+        have = deg > 0;
+      }
+    }
+    // warp-aggregated append to queue t+1
+    const unsigned mask = __ballot_sync(0xffffffffu, have);
+    if (mask) {
+      long long d = have ? deg : 0;
+      const long long inc = warp_inclusive_scan(d);
+      unsigned long long old = 0;
+      if (lane == 31) old = atomicAdd(&p.ctl->q[qn], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
+      old = __shfl_sync(0xffffffffu, old, 31);
+      if (have) {
+        const unsigned slot = (unsigned)(old & kCountMask) + __popc(mask & ((1u << lane) - 1));
+        p.qids[qn][slot] = v;
+        p.qeb[qn][slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - d));
+      }
+    }
+  }
+  act = __reduce_or_sync(0xffffffffu, (unsigned)act) | ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(act >> 32)) << 32);
+  if (lane == 0 && act) atomicOr(&s_act, act);
+  __syncthreads();
+  if (threadIdx.x < kSlots && s_msum[threadIdx.x]) atomicAdd(&p.ctl->msum[threadIdx.x], s_msum[threadIdx.x]);
+  if (threadIdx.x == 0 && s_act) atomicOr(&p.ctl->active[t % kRing], s_act);
+}
+
+// Retire frontier t (clear its F entries) and reset the counters tick t+1
+// does not use any more.
+__global__ void k_sv_retire(Params p, long long t) {
+  const int qs = (int)(t % 3);
+  const unsigned cnt = (unsigned)(ld_cg_u64(&p.ctl->q[qs]) & kCountMask);
+  unsigned long long* Fc = p.F[t & 1];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x)
+    Fc[p.qids[qs][i]] = 0ull;
+}
+
+__global__ void k_sv_reset(Params p, long long t) {
+  // before tick t: queue (t+1)%3 empty, touched counter of t empty, active slot of t empty
+  if (threadIdx.x == 0) {
+    p.ctl->q[(t + 1) % 3] = 0ull;
+    p.ctl->tcount[t & 1] = 0u;
+    p.ctl->active[t % kRing] = 0ull;
+  }
+}
+
+// Seed slot s at src for tick t (its frontier bit, its level 0, a queue entry).
+__global__ void k_sv_seed(Params p, long long t, int s, int src) {
+  if (threadIdx.x != 0) return;
+  const unsigned long long bit = 1ull << s;
+  p.vis[src] |= bit;
+  p.F[t & 1][src] |= bit;
+  if (p.out[s]) p.out[s][src] = 0;
+  p.ctl->msum[s] = 0;
+  const long long b0 = p.beg[src], d = p.beg[src + 1] - b0;
+  p.ctl->msum[s] = (unsigned long long)d;
+  if (d > 0) {
+    const unsigned long long old = atomicAdd(&p.ctl->q[t % 3], ((unsigned long long)d << 31) | 1ull);
+    p.qids[t % 3][old & kCountMask] = src;
+    p.qeb[t % 3][old & kCountMask] = (unsigned)(old >> 31);
+  }
+}
+
+// Clear the visited bits of retired slots.
+__global__ void k_sv_clear(Params p, unsigned long long mask) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < p.V; v += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long x = p.vis[v];
+    if (x & mask) p.vis[v] = x & ~mask;
+  }
+}
+
+}  // namespace sv
+
+struct ServeRequest {
+  int graph;
+  int src;
+  double arrival_us;
+  double admit_us = -1, finish_us = -1;
+  int slot = -1;
+  int* out = nullptr;     // device output (int32[V])
+  long long join = 0;
+  int status = 0;         // 0 waiting, 1 running, 2 done
+  unsigned long long msum = 0;
+};
+
+struct SlotBatch {
+  Graph* g = nullptr;
+  cudaStream_t stream = nullptr;
+  DevBuf vis, F0, F1, N, touched, tlist, q[3], qe[3], ctl, out_tab, join_tab;
+  sv::Params p;
+  long long tick = 0;
+  int req_of_slot[sv::kSlots];
+  unsigned long long busy = 0;
+  std::deque<int> waiting;
+  int k_ticks = 1;
+  std::vector<int> depths;
+  int grid = 0;
+};
+
+struct Server {
+  int device = 0;
+  std::vector<std::unique_ptr<SlotBatch>> batches;
+  size_t budget = 0, in_use = 0;
+  cudaMemPool_t pool = nullptr;
+  int keep_outputs = 0;
+  std::vector<ServeRequest> reqs;
+  ~Server() {
+    DeviceGuard dg(device);
+    for (auto& b : batches)
+      if (b->stream) {
+        cudaStreamSynchronize(b->stream);
+        cudaStreamDestroy(b->stream);
+      }
+  }
+};
+
+static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
+  b.g = g;
+  const long long V = g->V, nw = (V + 31) / 32 + 64;
+  xbfs_status st;
+  if ((st = b.vis.ensure(V * 8)) || (st = b.F0.ensure(V * 8)) || (st = b.F1.ensure(V * 8)) || (st = b.N.ensure(V * 8)) ||
+      (st = b.touched.ensure(nw * 4)) || (st = b.tlist.ensure(V * 4 + 4)) || (st = b.ctl.ensure(sizeof(sv::Ctl))) ||
+      (st = b.out_tab.ensure(sizeof(int*) * sv::kSlots)) || (st = b.join_tab.ensure(8 * sv::kSlots)))
+    return st;
+  // a tick's queue holds at most V merged vertices plus the seeds of one round
+  for (int i = 0; i < 3; ++i)
+    if ((st = b.q[i].ensure((V + sv::kSlots + 1) * 4)) || (st = b.qe[i].ensure((V + sv::kSlots + 1) * 4))) return st;
+  XBFS_CUDA_TRY(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
+  XBFS_CUDA_TRY(cudaMemsetAsync(b.vis.p, 0, V * 8, b.stream));
+  XBFS_CUDA_TRY(cudaMemsetAsync(b.F0.p, 0, V * 8, b.stream));
+  XBFS_CUDA_TRY(cudaMemsetAsync(b.F1.p, 0, V * 8, b.stream));
+  XBFS_CUDA_TRY(cudaMemsetAsync(b.N.p, 0, V * 8, b.stream));
+  XBFS_CUDA_TRY(cudaMemsetAsync(b.touched.p, 0, nw * 4, b.stream));
+  XBFS_CUDA_TRY(cudaMemsetAsync(b.ctl.p, 0, sizeof(sv::Ctl), b.stream));
+  XBFS_CUDA_TRY(cudaMemsetAsync(b.out_tab.p, 0, sizeof(int*) * sv::kSlots, b.stream));
+  XBFS_CUDA_TRY(cudaMemsetAsync(b.join_tab.p, 0, 8 * sv::kSlots, b.stream));
+  sv::Params& p = b.p;
+  p.beg = g->beg.as<long long>();
+  p.csr = g->csr.as<int>();
+  p.V = V;
+  p.vis = b.vis.as<unsigned long long>();
+  p.F[0] = b.F0.as<unsigned long long>();
+  p.F[1] = b.F1.as<unsigned long long>();
+  p.N = b.N.as<unsigned long long>();
+  p.touched = b.touched.as<uint32_t>();
+  p.tlist = b.tlist.as<int>();
+  for (int i = 0; i < 3; ++i) {
+    p.qids[i] = b.q[i].as<int>();
+    p.qeb[i] = b.qe[i].as<unsigned>();
+  }
+  p.out = b.out_tab.as<int* const>();
+  p.join = b.join_tab.as<long long>();
+  p.ctl = b.ctl.as<sv::Ctl>();
+  for (int s = 0; s < sv::kSlots; ++s) b.req_of_slot[s] = -1;
+  b.grid = nsm * 4;
+  return XBFS_OK;
+}
+
+static xbfs_status batch_ticks(SlotBatch& b, int k) {
+  for (int i = 0; i < k; ++i) {
+    const long long t = b.tick + i;
+    sv::k_sv_reset<<<1, 32, 0, b.stream>>>(b.p, t);
+    sv::k_sv_expand<<<b.grid, sv::kBlock, 0, b.stream>>>(b.p, t);
+    sv::k_sv_merge<<<b.grid, sv::kBlock, 0, b.stream>>>(b.p, t);
+    sv::k_sv_retire<<<b.grid, 256, 0, b.stream>>>(b.p, t);
+  }
+  XBFS_CUDA_TRY(cudaGetLastError());
+  return XBFS_OK;
+}
+
+static double now_us(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace xbfs
+
+using namespace xbfs;
+
+extern "C" {
+
+xbfs_status xbfs_serve_create(xbfs_graph* const* graphs, int32_t n, int32_t device, int64_t hbm_budget_bytes,
+                              xbfs_server** out) {
+  if (!graphs || n <= 0 || !out) return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
+  *out = nullptr;
+  DeviceGuard dg(device);
+  std::unique_ptr<Server> srv(new Server());
+  srv->device = device;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  for (int i = 0; i < n; ++i) {
+    Graph* g = (Graph*)graphs[i];
+    if (!g || g->device != device) return set_error(XBFS_ERR_INVALID_ARG, "graph %d missing or on another device", i);
+    if (g->E >= (1ll << 32)) return set_error(XBFS_ERR_UNSUPPORTED, "graph %d needs E < 2^32", i);
+    std::unique_ptr<SlotBatch> b(new SlotBatch());
+    xbfs_status st = batch_init(*b, g, nsm);
+    if (st) return st;
+    srv->batches.push_back(std::move(b));
+  }
+  size_t fr = 0, tot = 0;
+  XBFS_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+  const size_t reserve = (size_t)2 << 30;
+  srv->budget = hbm_budget_bytes > 0 ? (size_t)hbm_budget_bytes : (fr > reserve ? fr - reserve : fr / 2);
+  XBFS_CUDA_TRY(cudaDeviceGetDefaultMemPool(&srv->pool, device));
+  uint64_t thr = UINT64_MAX;
+  XBFS_CUDA_TRY(cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  XBFS_CUDA_TRY(cudaDeviceSynchronize());
+  *out = (xbfs_server*)srv.release();
+  return XBFS_OK;
+}
+
+// Runs a whole request trace in real time: request i (graph[i], src[i])
+// arrives arrival_us[i] microseconds after the start. Outputs: admit / finish
+// times (us since start) and the Graph500 edge count of each request. With
+// keep_outputs, levels[i] receives a device pointer to request i's int32[V]
+// level array (release with xbfs_serve_release); otherwise outputs are freed
+// as requests finish. *wall_us = time from start to the last completion.
+xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, const int32_t* src,
+                           const double* arrival_us, int32_t keep_outputs, double* admit_us, double* finish_us,
+                           int64_t* edges_mc, int32_t** levels, double* wall_us) {
+  Server* srv = (Server*)sh;
+  if (!srv || n < 0 || (n > 0 && (!graph || !src || !arrival_us || !admit_us || !finish_us))) {
+    return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
+  }
+  if (keep_outputs && !levels) return set_error(XBFS_ERR_INVALID_ARG, "keep_outputs needs levels[]");
+  DeviceGuard dg(srv->device);
+  const int nb = (int)srv->batches.size();
+  srv->reqs.assign(n, ServeRequest());
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) {
+    if (graph[i] < 0 || graph[i] >= nb) return set_error(XBFS_ERR_INVALID_ARG, "request %d: bad graph", i);
+    if (src[i] < 0 || src[i] >= srv->batches[graph[i]]->g->V)
+      return set_error(XBFS_ERR_INVALID_ARG, "request %d: source out of range", i);
+    srv->reqs[i].graph = graph[i];
+    srv->reqs[i].src = src[i];
+    srv->reqs[i].arrival_us = arrival_us[i];
+    order[i] = i;
+  }
+  for (int i = 0; i < n; ++i)
+    if ((size_t)srv->batches[graph[i]]->g->V * 4 > srv->budget)
+      return set_error(XBFS_ERR_OOM, "request %d: its level array does not fit the HBM budget", i);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return arrival_us[a] < arrival_us[b]; });
+  const auto t0 = std::chrono::steady_clock::now();
+  size_t next = 0;
+  int done = 0;
+  std::vector<sv::Ctl> hctl(nb);
+  const double last_arrival = n ? srv->reqs[order.back()].arrival_us : 0.0;
+  while (done < n) {
+    const double now = now_us(t0);
+    if (now > last_arrival + 1200e6)
+      return set_error(XBFS_ERR_DEVICE_TIMEOUT, "serving loop made no progress for 20 minutes");
+    // arrivals
+    while (next < order.size() && srv->reqs[order[next]].arrival_us <= now) {
+      srv->batches[srv->reqs[order[next]].graph]->waiting.push_back(order[next]);
+      ++next;
+    }
+    // admission: a free slot and room in the HBM budget
+    for (int gi = 0; gi < nb; ++gi) {
+      SlotBatch& b = *srv->batches[gi];
+      while (!b.waiting.empty() && b.busy != ~0ull) {
+        const size_t need = (size_t)b.g->V * 4;
+        if (srv->in_use + need > srv->budget) break;
+        const int ri = b.waiting.front();
+        b.waiting.pop_front();
+        ServeRequest& r = srv->reqs[ri];
+        const int s = __builtin_ctzll(~b.busy);
+        b.busy |= 1ull << s;
+        b.req_of_slot[s] = ri;
+        void* mem = nullptr;
+        XBFS_CUDA_TRY(cudaMallocFromPoolAsync(&mem, need, srv->pool, b.stream));
+        srv->in_use += need;
+        r.out = (int*)mem;
+        r.slot = s;
+        r.join = b.tick;
+        r.admit_us = now_us(t0);
+        r.status = 1;
+        XBFS_CUDA_TRY(cudaMemsetAsync(r.out, 0xff, need, b.stream));
+        XBFS_CUDA_TRY(cudaMemcpyAsync(b.out_tab.as<int*>() + s, &r.out, sizeof(int*), cudaMemcpyHostToDevice, b.stream));
+        XBFS_CUDA_TRY(cudaMemcpyAsync(b.join_tab.as<long long>() + s, &r.join, 8, cudaMemcpyHostToDevice, b.stream));
+        // the seed goes into tick b.tick's frontier
+        sv::k_sv_seed<<<1, 32, 0, b.stream>>>(b.p, b.tick, s, r.src);
+      }
+    }
+    // advance every batch with running slots by K ticks (overlapping streams)
+    int running = 0;
+    for (int gi = 0; gi < nb; ++gi) {
+      SlotBatch& b = *srv->batches[gi];
+      if (!b.busy) continue;
+      ++running;
+      const int k = std::max(1, std::min(b.k_ticks, sv::kRing - (int)(b.tick % sv::kRing)));
+      xbfs_status st = batch_ticks(b, k);
+      if (st) return st;
+      XBFS_CUDA_TRY(cudaMemcpyAsync(&hctl[gi], b.ctl.p, sizeof(sv::Ctl), cudaMemcpyDeviceToHost, b.stream));
+      b.depths.push_back(k);  // ticks issued this round
+    }
+    if (!running) {
+      if (next < order.size()) {
+        const double wait = srv->reqs[order[next]].arrival_us - now_us(t0);
+        if (wait > 50) {
+          // idle until the next arrival (short sleeps keep latency honest)
+          const auto until = t0 + std::chrono::microseconds((long long)srv->reqs[order[next]].arrival_us);
+          while (std::chrono::steady_clock::now() < until) {
+          }
+        }
+      }
+      continue;
+    }
+    for (int gi = 0; gi < nb; ++gi) {
+      SlotBatch& b = *srv->batches[gi];
+      if (!b.busy) continue;
+      XBFS_CUDA_TRY(cudaStreamSynchronize(b.stream));
+      const int k = b.depths.back();
+      b.depths.pop_back();
+      unsigned long long finished = 0;
+      for (int i = 0; i < k; ++i) {
+        const long long t = b.tick + i;
+        const unsigned long long act = hctl[gi].active[t % sv::kRing];
+        // slots joined at or before t that gained nothing at t are complete
+        for (unsigned long long m = b.busy & ~finished; m; m &= m - 1) {
+          const int s = __builtin_ctzll(m);
+          const ServeRequest& r = srv->reqs[b.req_of_slot[s]];
+          if (r.join <= t && !((act >> s) & 1ull)) finished |= 1ull << s;
+        }
+      }
+      b.tick += k;
+      if (!finished) {
+        b.k_ticks = std::min(sv::kRing, b.k_ticks * 2);
+        continue;
+      }
+      const double tf = now_us(t0);
+      int max_depth = 0;
+      for (unsigned long long m = finished; m; m &= m - 1) {
+        const int s = __builtin_ctzll(m);
+        ServeRequest& r = srv->reqs[b.req_of_slot[s]];
+        r.finish_us = tf;
+        r.status = 2;
+        r.msum = hctl[gi].msum[s];
+        max_depth = std::max<int>(max_depth, (int)(b.tick - r.join));
+        if (!srv->keep_outputs && !keep_outputs) {
+          XBFS_CUDA_TRY(cudaFreeAsync(r.out, b.stream));
+          srv->in_use -= (size_t)b.g->V * 4;
+          r.out = nullptr;
+        }
+        int* null = nullptr;
+        XBFS_CUDA_TRY(cudaMemcpyAsync(b.out_tab.as<int*>() + s, &null, sizeof(int*), cudaMemcpyHostToDevice, b.stream));
+        b.req_of_slot[s] = -1;
+        ++done;
+      }
+      sv::k_sv_clear<<<b.grid, 256, 0, b.stream>>>(b.p, finished);
+      XBFS_CUDA_TRY(cudaGetLastError());
+      b.busy &= ~finished;
+      // host every ~1/8 of the depth seen so far, at least every tick
+      b.k_ticks = std::max(1, std::min(sv::kRing, max_depth / 8));
+    }
+  }
+  for (auto& b : srv->batches) XBFS_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  if (wall_us) *wall_us = now_us(t0);
+  for (int i = 0; i < n; ++i) {
+    admit_us[i] = srv->reqs[i].admit_us;
+    finish_us[i] = srv->reqs[i].finish_us;
+    if (edges_mc) edges_mc[i] = (int64_t)(srv->reqs[i].msum / 2);
+    if (keep_outputs) levels[i] = srv->reqs[i].out;
+  }
+  return XBFS_OK;
+}
+
+xbfs_status xbfs_serve_release(xbfs_server* sh, int32_t* levels_dev, int64_t V) {
+  Server* srv = (Server*)sh;
+  if (!srv || !levels_dev) return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
+  DeviceGuard dg(srv->device);
+  XBFS_CUDA_TRY(cudaFreeAsync(levels_dev, srv->batches[0]->stream));
+  XBFS_CUDA_TRY(cudaStreamSynchronize(srv->batches[0]->stream));
+  srv->in_use -= std::min<size_t>(srv->in_use, (size_t)V * 4);
+  return XBFS_OK;
+}
+
+// Copies a kept level array to host memory and releases it.
+xbfs_status xbfs_serve_fetch(xbfs_server* sh, int32_t* levels_dev, int64_t V, int32_t* host_out) {
+  Server* srv = (Server*)sh;
+  if (!srv || !levels_dev || !host_out || V <= 0) return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
+  DeviceGuard dg(srv->device);
+  XBFS_CUDA_TRY(cudaMemcpy(host_out, levels_dev, (size_t)V * 4, cudaMemcpyDeviceToHost));
+  return xbfs_serve_release(sh, levels_dev, V);
+}
+
+void xbfs_serve_free(xbfs_server* sh) { delete (Server*)sh; }
+
+}  // extern "C"
