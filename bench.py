@@ -137,7 +137,10 @@ def ncu_traffic(workload_tag: str):
 
 
 # ---------------------------------------------------------------------------
-def dist_init():
+def dist_init(backend: str = "nccl"):
+    """One process per GPU under torchrun; the process group only carries the
+    scalar reductions of the job-wide figures (no data-path collective: every
+    rank traverses its own replica of the graph). ``gloo`` serves CPU tests."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -146,18 +149,32 @@ def dist_init():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
 def allreduce(vals, op):
     import torch
     import torch.distributed as dist
-    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=op)
     return t.tolist()
+
+
+def job_rate(edges: float, my_seconds: float, world: int):
+    """Whole-job GTEPS of independent replicas: the edges of all ranks over the
+    slowest rank's time. Returns (gteps, total edges, max seconds)."""
+    if world > 1:
+        import torch.distributed as dist
+        edges, = allreduce([float(edges)], dist.ReduceOp.SUM)
+        my_seconds, = allreduce([float(my_seconds)], dist.ReduceOp.MAX)
+    return float(edges) / my_seconds / 1e9, float(edges), float(my_seconds)
 
 
 def barrier(world):
@@ -244,13 +261,8 @@ def run_ours(args):
     step_ms = [a.elapsed_time(b) for a, b in evs]
     kernel_ms = [r.kernel_ms for r in results]
     edges = sum(r.edges_mc for r in results)
-    my_ms = sum(step_ms)
-    if world > 1:
-        tot_edges, = allreduce([float(edges)], dist.ReduceOp.SUM)
-        max_ms, = allreduce([my_ms], dist.ReduceOp.MAX)
-    else:
-        tot_edges, max_ms = float(edges), my_ms
-    value = tot_edges / (max_ms * 1e-3) / 1e9
+    value, tot_edges, max_s = job_rate(edges, sum(step_ms) * 1e-3, world)
+    max_ms = max_s * 1e3
 
     # ---- end to end through the public API with host buffers
     e2e = None
@@ -265,11 +277,8 @@ def run_ours(args):
             r = g.bfs(int(srcs[i % len(srcs)]), levels=host_lv, opts=opts)
             e_edges += r.edges_mc
         barrier(world)
-        e_s = time.perf_counter() - t0
-        if world > 1:
-            e_edges, = allreduce([float(e_edges)], dist.ReduceOp.SUM)
-            e_s, = allreduce([e_s], dist.ReduceOp.MAX)
-        e2e = {"value": round(e_edges / e_s / 1e9, 3), "unit": "GTEPS",
+        e_gteps, _, _ = job_rate(e_edges, time.perf_counter() - t0, world)
+        e2e = {"value": round(e_gteps, 3), "unit": "GTEPS",
                "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * V,
                "note": "xbfs_bfs with a pinned host level array: D2H of int32[V] levels per step; "
                        "the source id travels in the launch parameters; graph resident in HBM"}
