@@ -193,8 +193,12 @@ xbfs_status xbfs_serve_create(xbfs_graph* const* graphs, int32_t n, int32_t devi
 /* Replays a request trace in real time (request i targets graph[i] from
  * src[i] and arrives arrival_us[i] after the start). Returns per request the
  * admission and completion times (us since start) and its Graph500 edge
- * count; with keep_outputs, levels[i] = device pointer to its level array
- * (free with xbfs_serve_release). */
+ * count. keep_outputs = 0: level arrays are freed as requests finish;
+ * 1: levels[i] receives a device pointer to request i's level array (free
+ * with xbfs_serve_release; kept arrays count against the HBM budget, and a
+ * request they block is an XBFS_ERR_OOM); 2: levels[i] is the caller's host
+ * array of V int32 that receives the levels when request i finishes (its
+ * device array is freed at once). */
 xbfs_status xbfs_serve_run(xbfs_server* s, int32_t n, const int32_t* graph, const int32_t* src,
                            const double* arrival_us, int32_t keep_outputs, double* admit_us, double* finish_us,
                            int64_t* edges_mc, int32_t** levels, double* wall_us);

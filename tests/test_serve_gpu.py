@@ -50,12 +50,32 @@ def test_results_in_the_mix_equal_results_alone(rate):
 
 
 def test_more_requests_than_slots_and_a_tight_memory_budget():
+    """More than 64 requests per graph at once, and an HBM budget for three
+    level arrays at a time: requests wait for slots and memory, results are
+    delivered to host arrays as they finish (freeing their device memory)."""
     cpu, graphs = setup(1)
     gid, src, arr = trace(cpu, 300, 1e8, 2)   # everything arrives at once: > 64 per graph
     budget = 3 * max(g.V for g in graphs) * 4   # room for three outputs at a time
     srv = Server(graphs, hbm_budget_bytes=budget)
-    res = srv.run(gid, src, arr, keep_outputs=True)
-    check_all(srv, cpu, graphs, gid, src, res)
+    res = srv.run(gid, src, arr, to_host=True)
+    assert len(set(res["admit_us"].tolist())) > 1   # admission waited for memory
+    for i, (g, s) in enumerate(zip(gid, src)):
+        ref = oracle.bfs_queue(cpu[g][0], cpu[g][1], int(s))
+        assert np.array_equal(res["levels"][i], ref), f"request {i} (graph {g}, source {s}) differs"
+        assert res["edges_mc"][i] == oracle.edges_mc(cpu[g][0], ref)
+
+
+def test_kept_outputs_that_fill_the_budget_are_an_error():
+    """Device-kept outputs hold their memory until released: when they block
+    a waiting request the run stops with XBFS_ERR_OOM instead of waiting."""
+    from xbfs_b200._lib import XBFS_ERR_OOM, XbfsError
+    cpu, graphs = setup(1)
+    gid, src, arr = trace(cpu, 20, 1e8, 5)
+    budget = 3 * max(g.V for g in graphs) * 4
+    srv = Server(graphs, hbm_budget_bytes=budget)
+    with pytest.raises(XbfsError) as e:
+        srv.run(gid, src, arr, keep_outputs=True)
+    assert e.value.status == XBFS_ERR_OOM and "fill the HBM budget" in e.value.detail
 
 
 def test_run_without_keeping_outputs_reports_edges():

@@ -362,7 +362,10 @@ class Server:
         self._h = h
         self.graphs = list(graphs)
 
-    def run(self, graph_ids, srcs, arrival_us, keep_outputs: bool = False) -> dict:
+    def run(self, graph_ids, srcs, arrival_us, keep_outputs: bool = False, to_host: bool = False) -> dict:
+        """Replay a request trace. ``keep_outputs``: return device level arrays
+        (``levels_dev``, read with fetch()); ``to_host``: each finished request's
+        levels are copied to a host array (``levels``) and its device memory freed."""
         g = np.ascontiguousarray(graph_ids, dtype=np.int32)
         s = np.ascontiguousarray(srcs, dtype=np.int32)
         a = np.ascontiguousarray(arrival_us, dtype=np.float64)
@@ -371,17 +374,25 @@ class Server:
         fin = np.zeros(n, dtype=np.float64)
         mc = np.zeros(n, dtype=np.int64)
         ptrs = (C.c_void_p * max(n, 1))()
+        mode = 2 if to_host else (1 if keep_outputs else 0)
+        host = []
+        if to_host:
+            host = [np.empty(self.graphs[int(gi)].V, dtype=np.int32) for gi in g]
+            for i, h in enumerate(host):
+                ptrs[i] = h.ctypes.data
         wall = C.c_double(0)
-        check(lib.xbfs_serve_run(self._h, n, g.ctypes.data, s.ctypes.data, a.ctypes.data, 1 if keep_outputs else 0,
+        check(lib.xbfs_serve_run(self._h, n, g.ctypes.data, s.ctypes.data, a.ctypes.data, mode,
                                  admit.ctypes.data, fin.ctypes.data, mc.ctypes.data,
-                                 C.cast(ptrs, C.c_void_p) if keep_outputs else None, C.byref(wall)))
+                                 C.cast(ptrs, C.c_void_p) if mode else None, C.byref(wall)))
         lat = fin - a
         out = {"admit_us": admit, "finish_us": fin, "latency_us": lat, "edges_mc": mc, "wall_us": wall.value,
                "p50_us": float(np.percentile(lat, 50)) if n else 0.0,
                "p99_us": float(np.percentile(lat, 99)) if n else 0.0,
                "gteps": float(mc.sum() / (wall.value * 1e-6) / 1e9) if wall.value > 0 else 0.0}
-        if keep_outputs:
+        if mode == 1:
             out["levels_dev"] = [ptrs[i] for i in range(n)]
+        if mode == 2:
+            out["levels"] = host
         return out
 
     def fetch(self, ptr: int, V: int) -> np.ndarray:

@@ -293,7 +293,6 @@ struct Server {
   std::vector<std::unique_ptr<SlotBatch>> batches;
   size_t budget = 0, in_use = 0;
   cudaMemPool_t pool = nullptr;
-  int keep_outputs = 0;
   std::vector<ServeRequest> reqs;
   ~Server() {
     DeviceGuard dg(device);
@@ -402,9 +401,10 @@ xbfs_status xbfs_serve_create(xbfs_graph* const* graphs, int32_t n, int32_t devi
 // Runs a whole request trace in real time: request i (graph[i], src[i])
 // arrives arrival_us[i] microseconds after the start. Outputs: admit / finish
 // times (us since start) and the Graph500 edge count of each request. With
-// keep_outputs, levels[i] receives a device pointer to request i's int32[V]
-// level array (release with xbfs_serve_release); otherwise outputs are freed
-// as requests finish. *wall_us = time from start to the last completion.
+// keep_outputs = 1, levels[i] receives a device pointer to request i's
+// int32[V] level array (release with xbfs_serve_release); with 2, levels[i]
+// is the caller's host array that receives the levels when the request
+// finishes; otherwise outputs are freed as requests finish. *wall_us = time from start to the last completion.
 xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, const int32_t* src,
                            const double* arrival_us, int32_t keep_outputs, double* admit_us, double* finish_us,
                            int64_t* edges_mc, int32_t** levels, double* wall_us) {
@@ -412,7 +412,11 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
   if (!srv || n < 0 || (n > 0 && (!graph || !src || !arrival_us || !admit_us || !finish_us))) {
     return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
   }
+  if (keep_outputs < 0 || keep_outputs > 2) return set_error(XBFS_ERR_INVALID_ARG, "keep_outputs must be 0, 1 or 2");
   if (keep_outputs && !levels) return set_error(XBFS_ERR_INVALID_ARG, "keep_outputs needs levels[]");
+  if (keep_outputs == 2)
+    for (int i = 0; i < n; ++i)
+      if (!levels[i]) return set_error(XBFS_ERR_INVALID_ARG, "request %d: no host level array", i);
   DeviceGuard dg(srv->device);
   const int nb = (int)srv->batches.size();
   srv->reqs.assign(n, ServeRequest());
@@ -484,6 +488,14 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
       b.depths.push_back(k);  // ticks issued this round
     }
     if (!running) {
+      // nothing runs, so nothing will give memory back: a request that has
+      // arrived and still waits can only be blocked by kept outputs
+      for (int gi = 0; gi < nb; ++gi)
+        if (!srv->batches[gi]->waiting.empty())
+          return set_error(XBFS_ERR_OOM,
+                           "kept level arrays (%zu bytes) fill the HBM budget (%zu bytes): release them, or run "
+                           "with keep_outputs = 0 or 2",
+                           srv->in_use, srv->budget);
       if (next < order.size()) {
         const double wait = srv->reqs[order[next]].arrival_us - now_us(t0);
         if (wait > 50) {
@@ -526,7 +538,10 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
         r.status = 2;
         r.msum = hctl[gi].msum[s];
         max_depth = std::max<int>(max_depth, (int)(b.tick - r.join));
-        if (!srv->keep_outputs && !keep_outputs) {
+        if (keep_outputs == 2)  // deliver to the caller's host array, then give the memory back
+          XBFS_CUDA_TRY(cudaMemcpyAsync(levels[b.req_of_slot[s]], r.out, (size_t)b.g->V * 4, cudaMemcpyDeviceToHost,
+                                        b.stream));
+        if (keep_outputs != 1) {
           XBFS_CUDA_TRY(cudaFreeAsync(r.out, b.stream));
           srv->in_use -= (size_t)b.g->V * 4;
           r.out = nullptr;
@@ -549,7 +564,7 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
     admit_us[i] = srv->reqs[i].admit_us;
     finish_us[i] = srv->reqs[i].finish_us;
     if (edges_mc) edges_mc[i] = (int64_t)(srv->reqs[i].msum / 2);
-    if (keep_outputs) levels[i] = srv->reqs[i].out;
+    if (keep_outputs == 1) levels[i] = srv->reqs[i].out;
   }
   return XBFS_OK;
 }
