@@ -152,6 +152,33 @@ void xbfs_graph_free(xbfs_graph* g);
 xbfs_status xbfs_bfs(xbfs_graph* g, int32_t src, int32_t* levels, int32_t* parents,
                      const xbfs_opts* opts, xbfs_stats* stats);
 
+/* Allocation-free single-source BFS. No counterpart in the reference (its
+ * main cudaMallocs the status arrays and queues itself); added for callers
+ * that may not allocate device memory while they traverse: a process whose
+ * HBM is pre-divided by its own pool or arena, or a latency-bound loop in
+ * which cudaMalloc/cudaFree would stall the device. Same kernel, options and
+ * results as xbfs_bfs, but the traversal workspace comes from one fixed
+ * static device array of XBFS_NOALLOC_SCRATCH_BYTES per device, not from
+ * cudaMalloc. Requirements and limits:
+ *  - levels (and parents, if not NULL) must be device memory on g's device;
+ *  - graphs whose workspace exceeds the array are refused with
+ *    XBFS_ERR_UNSUPPORTED and a message giving the bytes needed (R-MAT with
+ *    edge factor 16 fits up to about 2^20 vertices; xbfs_bfs has no limit);
+ *  - the first call on a device resolves the array's address
+ *    (cudaGetSymbolAddress, which also makes the runtime load the module
+ *    holding the array) and sets the kernel's launch attributes; make that
+ *    first call before any stream capture begins;
+ *  - nothing in the array has to start at zero: each call clears the
+ *    visited/frontier bitmaps and the control block it reads first;
+ *  - calls on the same device share the one array: calls that overlap in time
+ *    (other threads, other streams) race and corrupt each other's traversal.
+ *    Serialise them;
+ *  - the call waits for its stream to read back the status; opts->trace is
+ *    refused and stats->device_ms / kernel_ms are 0 (no events are created). */
+#define XBFS_NOALLOC_SCRATCH_BYTES (64ull << 20)
+xbfs_status xbfs_bfs_noalloc(xbfs_graph* g, int32_t src, int32_t* levels, int32_t* parents,
+                             const xbfs_opts* opts, xbfs_stats* stats);
+
 /* Batched multi-source BFS: n sources, levels = n x V int32 (source-major,
  * host or device). Sources are traversed 64 per uint64 word, up to 8 words
  * (512 sources) per pass. No counterpart in the reference (one source per

@@ -51,6 +51,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <mutex>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -1324,6 +1325,233 @@ xbfs_status level_costs(Graph* g, int32_t src, int32_t follow, int32_t cap, floa
   return XBFS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free traversal. Callers that must not allocate device memory at
+// traversal time: processes whose device memory is pre-divided by an arena or
+// pool that owns nearly all of HBM (a cudaMalloc beside it fails or fragments
+// the pool), and latency-bound service loops in which cudaMalloc/cudaFree
+// would stall the device (cudaFree synchronises it). They load the graph once
+// at start-up and then traverse with this path, which takes the k_bfs
+// workspace from the fixed array of static_scratch.cu instead of the per-graph
+// workspace that bfs_single grows with cudaMalloc. The launch is the same
+// kernel with the same parameters; only where the workspace lives differs.
+//
+// Layout of the scratch (each region 256-byte aligned), for a graph of V
+// vertices, nw = ceil(V/32) + 64 bitmap words:
+//   bits    5 * nw * 4      visited + 4 frontier bitmaps   cleared every call
+//   ctl     sizeof(Ctl)     barrier, descriptors, counters cleared every call
+//   rs      sizeof(ResumeState)                            unused (no stepping)
+//   ulist   nw * 32 * 4     bottom-up vertex lists         written before read
+//   heavy   3 arrays, (vertices of degree > 16) + 1 each   written before read
+//   queues  2 parities x 3 bins x (cap + 1) x (4 + 4 + 8)  written before read
+//   forced  n_forced bytes (forced policy only)            copied every call
+// No per-level history is kept (hist_cap = 0), so trace is not available.
+// ---------------------------------------------------------------------------
+extern cudaError_t noalloc_scratch_address(void** ptr);
+
+namespace {
+
+struct NoallocDevice {
+  bool ready = false;
+  unsigned char* scratch = nullptr;
+  int grid[2] = {0, 0};  // resident CTAs of k_bfs<false>, k_bfs<true>
+};
+std::mutex g_noalloc_mu;
+NoallocDevice g_noalloc[64];
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Per-device set-up, run once with `device` current: the scratch address and
+// the launch shape of both kernel instantiations.
+xbfs_status noalloc_setup(int device, NoallocDevice** out) {
+  if (device < 0 || device >= 64) return set_error(XBFS_ERR_INVALID_ARG, "device %d out of range", device);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  NoallocDevice& d = g_noalloc[device];
+  if (!d.ready) {
+    void* ptr = nullptr;
+    const cudaError_t e = noalloc_scratch_address(&ptr);
+    if (e != cudaSuccess || !ptr)
+      return set_error(XBFS_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed on device %d: %s",
+                       device, cudaGetErrorString(e));
+    int nsm = 0;
+    XBFS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    const void* fns[2] = {(const void*)k_bfs<false>, (const void*)k_bfs<true>};
+    for (int i = 0; i < 2; ++i) {
+      XBFS_CUDA_TRY(cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)));
+      int per_sm = 0;
+      XBFS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fns[i], kBlock, sizeof(Smem)));
+      if (per_sm < 1) return set_error(XBFS_ERR_INTERNAL, "traversal kernel cannot be resident");
+      d.grid[i] = nsm * per_sm;
+    }
+    d.scratch = (unsigned char*)ptr;
+    d.ready = true;
+  }
+  *out = &d;
+  return XBFS_OK;
+}
+
+}  // namespace
+
+xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents, const xbfs_opts* uopts,
+                        xbfs_stats* stats) {
+  const auto t_start = std::chrono::steady_clock::now();
+  xbfs_opts o;
+  xbfs_opts_init(&o);
+  if (uopts) {
+    if (uopts->struct_size != (int32_t)sizeof(xbfs_opts))
+      return set_error(XBFS_ERR_INVALID_ARG, "xbfs_opts.struct_size = %d, expected %zu (call xbfs_opts_init)",
+                       uopts->struct_size, sizeof(xbfs_opts));
+    o = *uopts;
+  }
+  if (!g) return set_error(XBFS_ERR_INVALID_ARG, "graph is NULL");
+  if (!levels) return set_error(XBFS_ERR_INVALID_ARG, "levels is NULL");
+  if (src < 0 || (int64_t)src >= g->V)
+    return set_error(XBFS_ERR_INVALID_ARG, "source %d out of range [0, %lld)", src, (long long)g->V);
+  if (g->E >= (1ll << 32))
+    return set_error(XBFS_ERR_UNSUPPORTED, "single-source path needs E < 2^32 (E = %lld)", (long long)g->E);
+  if (o.padding != 1) return set_error(XBFS_ERR_INVALID_ARG, "padding = %d: only 1 is supported", o.padding);
+  if (o.trace) return set_error(XBFS_ERR_UNSUPPORTED, "xbfs_bfs_noalloc keeps no per-level trace (trace = 1)");
+  if (o.small_max <= 0) o.small_max = 32;
+  if (o.medium_max < o.small_max) o.medium_max = o.small_max;
+  if (o.policy == XBFS_POLICY_FORCED && (!o.forced || o.n_forced <= 0))
+    return set_error(XBFS_ERR_INVALID_ARG, "forced policy needs a non-empty forced[] array");
+  if (o.policy < 0 || o.policy > 3) return set_error(XBFS_ERR_INVALID_ARG, "bad policy %d", o.policy);
+  if (!(o.alpha > 0)) o.alpha = 0.1f;
+
+  DeviceGuard dg(g->device);
+  if (!is_device_pointer(levels))
+    return set_error(XBFS_ERR_INVALID_ARG, "xbfs_bfs_noalloc needs levels in device memory");
+  if (parents && !is_device_pointer(parents))
+    return set_error(XBFS_ERR_INVALID_ARG, "xbfs_bfs_noalloc needs parents in device memory");
+  NoallocDevice* dev = nullptr;
+  xbfs_status st = noalloc_setup(g->device, &dev);
+  if (st) return st;
+
+  // ---- carve the scratch; refuse graphs whose workspace does not fit
+  const size_t nw = (size_t)((g->V + 31) / 32 + 64);
+  auto count_gt = [&](long long t) -> size_t {
+    if (t < 1) return (size_t)g->V;
+    int k = 0;
+    while (k < 15 && (1ll << (k + 1)) <= t) ++k;
+    return (size_t)g->cnt_deg_gt[k];
+  };
+  size_t cap[3];
+  cap[0] = (size_t)g->V;
+  cap[1] = std::min<size_t>((size_t)g->V, count_gt(o.small_max));
+  cap[2] = std::min<size_t>((size_t)g->V, count_gt(o.medium_max));
+  const size_t hcap = (size_t)g->cnt_deg_gt[4] + 1;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off = align256(off + bytes);
+    return at;
+  };
+  const size_t o_bits = take(nw * 4 * 5);
+  const size_t o_ctl = take(sizeof(Ctl));
+  const size_t o_rs = take(sizeof(ResumeState));
+  const size_t o_ulist = take(nw * 32 * 4);
+  const size_t o_hid = take(hcap * 4), o_heb = take(hcap * 4), o_hbg = take(hcap * 8);
+  size_t o_q[2][3][3];
+  for (int par = 0; par < 2; ++par)
+    for (int b = 0; b < 3; ++b) {
+      o_q[par][b][0] = take((cap[b] + 1) * 4);
+      o_q[par][b][1] = take((cap[b] + 1) * 4);
+      o_q[par][b][2] = take((cap[b] + 1) * 8);
+    }
+  const size_t o_forced = take(o.policy == XBFS_POLICY_FORCED ? (size_t)o.n_forced : 0);
+  if (off > (size_t)XBFS_NOALLOC_SCRATCH_BYTES)
+    return set_error(XBFS_ERR_UNSUPPORTED,
+                     "graph needs %zu bytes of traversal scratch (V = %lld); the static scratch of "
+                     "xbfs_bfs_noalloc holds %llu bytes (XBFS_NOALLOC_SCRATCH_BYTES): use xbfs_bfs",
+                     off, (long long)g->V, (unsigned long long)XBFS_NOALLOC_SCRATCH_BYTES);
+  unsigned char* base = dev->scratch;
+
+  // ---- kernel parameters: as setup_params, with the workspace in the scratch
+  Params p;
+  memset(&p, 0, sizeof(p));
+  p.beg = g->beg.as<long long>();
+  p.csr = g->csr.as<int>();
+  p.V = g->V;
+  p.E = g->E;
+  p.levels = levels;
+  p.parents = parents;
+  uint32_t* bits = (uint32_t*)(base + o_bits);
+  p.vis = bits;
+  for (int i = 0; i < 4; ++i) p.fb[i] = bits + (size_t)(i + 1) * nw;
+  for (int par = 0; par < 2; ++par)
+    for (int b = 0; b < 3; ++b) {
+      p.q[par][b].ids = (int*)(base + o_q[par][b][0]);
+      p.q[par][b].eb = (unsigned*)(base + o_q[par][b][1]);
+      p.q[par][b].bg = (long long*)(base + o_q[par][b][2]);
+    }
+  p.heavy.ids = (int*)(base + o_hid);
+  p.heavy.eb = (unsigned*)(base + o_heb);
+  p.heavy.bg = (long long*)(base + o_hbg);
+  p.ulist = (int*)(base + o_ulist);
+  p.ctl = (Ctl*)(base + o_ctl);
+  p.hist = nullptr;
+  p.hist_cap = 0;
+  p.forced = (signed char*)(base + o_forced);
+  p.n_forced = o.n_forced;
+  p.nwords = (g->V + 31) / 32;
+  p.n_ni = g->symmetric ? g->V - g->n_isolated : g->V;
+  p.policy = o.policy;
+  p.alpha = o.alpha;
+  p.async_bu = o.async_bu ? 1 : 0;
+  p.small_max = o.small_max;
+  p.medium_max = o.medium_max;
+  p.beamer_alpha = o.beamer_alpha > 0 ? o.beamer_alpha : 14.f;
+  p.beamer_beta = o.beamer_beta > 0 ? o.beamer_beta : 24.f;
+  p.timeout_ns = 10ull * 1000 * 1000 * 1000;
+  p.max_levels = g->V + 2;
+  extern const float* mlp_device_weights(int device);
+  p.mlp = mlp_device_weights(g->device);
+  if (o.policy == XBFS_POLICY_MLP && !p.mlp) p.policy = XBFS_POLICY_HEURISTIC;
+  p.allow_bu = g->symmetric ? 1 : 0;
+  p.rs = (ResumeState*)(base + o_rs);
+  p.bu_mode = o.reserved[0];
+  p.stop_level = LLONG_MAX;
+  p.resume = 0;
+  const bool par_on = parents != nullptr;
+  const void* kfn = par_on ? (const void*)k_bfs<true> : (const void*)k_bfs<false>;
+  int grid = dev->grid[par_on ? 1 : 0];
+  if (o.grid_dim > 0 && o.grid_dim < grid) grid = o.grid_dim;
+
+  // ---- initial state (the same steps as init_state) and the launch
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : g->stream;
+  XBFS_CUDA_TRY(cudaMemsetAsync(p.levels, 0xff, (size_t)g->V * 4, s));
+  if (par_on) XBFS_CUDA_TRY(cudaMemsetAsync(p.parents, 0xff, (size_t)g->V * 4, s));
+  XBFS_CUDA_TRY(cudaMemcpyAsync(p.vis, g->iso.p, nw * 4, cudaMemcpyDeviceToDevice, s));
+  XBFS_CUDA_TRY(cudaMemsetAsync(p.fb[0], 0, nw * 4 * 4, s));
+  XBFS_CUDA_TRY(cudaMemsetAsync(p.ctl, 0, sizeof(Ctl), s));
+  if (o.policy == XBFS_POLICY_FORCED)
+    XBFS_CUDA_TRY(cudaMemcpyAsync((void*)p.forced, o.forced, (size_t)o.n_forced, cudaMemcpyHostToDevice, s));
+  k_seed<<<1, 32, 0, s>>>(p, src, par_on ? 1 : 0);
+  XBFS_CUDA_TRY(cudaGetLastError());
+  void* args[] = {&p};
+  XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, sizeof(Smem), s));
+  Ctl hctl;
+  XBFS_CUDA_TRY(cudaMemcpyAsync(&hctl, p.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+  XBFS_CUDA_TRY(cudaStreamSynchronize(s));
+  if (hctl.err != 0)
+    return set_error((xbfs_status)hctl.err, "traversal kernel reported %s", xbfs_strerror(hctl.err));
+  if (stats) {
+    stats->struct_size = (int32_t)sizeof(xbfs_stats);
+    stats->depth = hctl.depth;
+    stats->reached = (int64_t)hctl.reached;
+    stats->edges_mc = (int64_t)(hctl.msum / 2);
+    stats->device_ms = 0.0;  // not timed: this path creates no CUDA events
+    stats->kernel_ms = 0.0;
+    stats->n_td_queue = hctl.strat_count[0];
+    stats->n_td_scan = hctl.strat_count[1];
+    stats->n_bu = hctl.strat_count[2];
+    stats->n_async = (int32_t)hctl.n_async;
+    stats->total_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  }
+  return XBFS_OK;
+}
+
 }  // namespace xbfs
 
 using namespace xbfs;
@@ -1333,6 +1561,11 @@ extern "C" {
 xbfs_status xbfs_bfs(xbfs_graph* gh, int32_t src, int32_t* levels, int32_t* parents, const xbfs_opts* opts,
                      xbfs_stats* stats) {
   return bfs_single((Graph*)gh, src, levels, parents, opts, stats);
+}
+
+xbfs_status xbfs_bfs_noalloc(xbfs_graph* gh, int32_t src, int32_t* levels, int32_t* parents,
+                             const xbfs_opts* opts, xbfs_stats* stats) {
+  return bfs_noalloc((Graph*)gh, src, levels, parents, opts, stats);
 }
 
 xbfs_status xbfs_level_costs(xbfs_graph* gh, int32_t src, int32_t follow, int32_t cap, float* costs,
