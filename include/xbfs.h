@@ -88,7 +88,16 @@ typedef struct xbfs_opts {
                            reference is wrong for padding > 1) */
   float beamer_alpha;   /* XBFS_POLICY_BEAMER: TD->BU when m_f > m_u/alpha (14) */
   float beamer_beta;    /*                     BU->TD when n_f < V/beta (24)   */
-  int32_t reserved[4];
+  int32_t bu_probe;     /* bottom-up neighbour loads: 0 = through L1 (default),
+                           1 = streaming (L1 bypass) */
+  int32_t wait_timeout_us; /* bound of every device-side wait of a traversal
+                              (grid barriers); 0 = 10 s. On expiry the call
+                              returns XBFS_ERR_DEVICE_TIMEOUT */
+  int32_t test_absent_block; /* failure-detection test hook: k > 0 makes CTA
+                                k-1 leave the traversal kernel before its first
+                                grid barrier, so the others' bounded wait runs
+                                out; 0 = off */
+  int32_t reserved;
 } xbfs_opts;
 
 typedef struct xbfs_stats {
@@ -151,6 +160,15 @@ void xbfs_graph_free(xbfs_graph* g);
  * cooperative launch); no per-level host round trip. */
 xbfs_status xbfs_bfs(xbfs_graph* g, int32_t src, int32_t* levels, int32_t* parents,
                      const xbfs_opts* opts, xbfs_stats* stats);
+
+/* n single-source traversals in one call (row i of levels, n x V int32, host
+ * or device, belongs to srcs[i]). Same kernel and results as n xbfs_bfs
+ * calls, pipelined: traversal i runs while the level array of traversal i-1
+ * is copied to host memory on a second stream. No reference counterpart
+ * (the reference runs one source per process); stats are summed over the
+ * traversals (depth = the largest), device_ms spans the whole pipeline. */
+xbfs_status xbfs_bfs_many(xbfs_graph* g, const int32_t* srcs, int32_t n, int32_t* levels,
+                          const xbfs_opts* opts, xbfs_stats* stats);
 
 /* Allocation-free single-source BFS. No counterpart in the reference (its
  * main cudaMallocs the status arrays and queues itself); added for callers
@@ -243,7 +261,10 @@ xbfs_status xbfs_last_trace(xbfs_graph* g, xbfs_level_trace* out, int32_t cap, i
  * reference's fixed heuristic stays the fallback).
  * xbfs_level_costs: for every level of a traversal from src, snapshot the
  * state, run the level once with each strategy (XBFS_TD_QUEUE, XBFS_TD_SCAN,
- * XBFS_BU) and record its device time in costs[level*3 + strategy] (us);
+ * XBFS_BU), then, from the state each one leaves, the next level once with
+ * each strategy (a strategy also decides whether the next frontier is a
+ * queue or a bitmap), and record the level's device time plus the cheapest
+ * next level's in costs[level*3 + strategy] (us);
  * continue along the cheapest (follow = 0) or the heuristic's choice
  * (follow = 1). trace[level] gets the level's statistics and the strategy
  * taken. *n = number of levels. Levels never depend on the strategies. */

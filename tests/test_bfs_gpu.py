@@ -181,3 +181,24 @@ def test_load_file_pair_and_malformed_inputs(tmp_path):
     with pytest.raises(XbfsError) as e:
         Graph.load(str(tmp_path / "c_beg.bin"), str(tmp_path / "c_csr.bin"))
     assert e.value.status == _lib.XBFS_ERR_FORMAT
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("out", ["host", "device"])
+def test_many_sources_pipelined_equal_single_calls(out):
+    """xbfs_bfs_many: n traversals with the level copies overlapped; every row
+    equals the oracle and the single-call result for its source."""
+    import torch
+    beg, csr = gen_rmat_host(15, 16, 31)
+    g = Graph.from_csr(beg, csr)
+    srcs = pick_sources(beg, 7, 5)
+    lv = None if out == "host" else torch.empty((len(srcs), g.V), dtype=torch.int32, device="cuda:0")
+    r = g.bfs_many(srcs, levels=lv)
+    rows = r.levels if out == "host" else r.levels.cpu().numpy()
+    mc = 0
+    for i, s in enumerate(srcs):
+        ref = oracle.bfs_queue(beg, csr, int(s))
+        assert np.array_equal(rows[i], ref), i
+        mc += oracle.edges_mc(beg, ref)
+    assert r.edges_mc == mc
+    g.free()

@@ -55,7 +55,10 @@ class Opts(C.Structure):
         ("padding", C.c_int32),
         ("beamer_alpha", C.c_float),
         ("beamer_beta", C.c_float),
-        ("reserved", C.c_int32 * 4),
+        ("bu_probe", C.c_int32),
+        ("wait_timeout_us", C.c_int32),
+        ("test_absent_block", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -119,6 +122,7 @@ SIGNATURES = {
     "xbfs_graph_free": (None, [_p]),
     "xbfs_bfs": (_i32, [_p, _i32, _p, _p, C.POINTER(Opts), C.POINTER(Stats)]),
     "xbfs_bfs_noalloc": (_i32, [_p, _i32, _p, _p, C.POINTER(Opts), C.POINTER(Stats)]),
+    "xbfs_bfs_many": (_i32, [_p, _p, _i32, _p, C.POINTER(Opts), C.POINTER(Stats)]),
     "xbfs_last_trace": (_i32, [_p, C.POINTER(LevelTrace), _i32, _PI32]),
     "xbfs_gen_rmat": (_i32, [_i32, _i32, _u64, _f64, _f64, _f64, _i32, C.POINTER(_p)]),
     "xbfs_gen_grid": (_i32, [_i32, _i32, _i32, C.POINTER(_p)]),

@@ -54,7 +54,9 @@ class BfsOptions:
     beamer_alpha: float = 14.0
     beamer_beta: float = 24.0
     stream: int = 0
-    bu_mode: int = 0   # bottom-up probe shape (xbfs_opts.reserved[0]); 0 = default
+    bu_mode: int = 0   # bottom-up neighbour loads (xbfs_opts.bu_probe): 0 = through L1, 1 = streaming
+    wait_timeout_us: int = 0     # bound of device-side waits; 0 = 10 s
+    test_absent_block: int = 0   # failure-detection test hook (xbfs_opts.test_absent_block)
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> Opts:
@@ -72,7 +74,9 @@ class BfsOptions:
         o.beamer_alpha = float(self.beamer_alpha)
         o.beamer_beta = float(self.beamer_beta)
         o.stream = self.stream or None
-        o.reserved[0] = int(self.bu_mode)
+        o.bu_probe = int(self.bu_mode)
+        o.wait_timeout_us = int(self.wait_timeout_us)
+        o.test_absent_block = int(self.test_absent_block)
         if self.forced is not None:
             vals = [STRATEGIES[s] if isinstance(s, str) else int(s) for s in self.forced]
             arr = (C.c_int8 * max(1, len(vals)))(*vals)
@@ -207,6 +211,27 @@ class Graph:
                          kernel_ms=st.kernel_ms,
                          strategies={"td_queue": st.n_td_queue, "td_scan": st.n_td_scan, "bu": st.n_bu},
                          n_async=st.n_async, trace=trace)
+
+    def bfs_many(self, srcs, levels=None, opts: Optional[BfsOptions] = None, **kw) -> BfsResult:
+        """One single-source traversal per source, pipelined with the copies of
+        their level arrays (xbfs_bfs_many): levels[i] belongs to srcs[i] (n x V
+        int32, numpy or CUDA tensor)."""
+        if opts is None:
+            opts = BfsOptions(**kw)
+        elif kw:
+            raise TypeError("pass either opts or keyword options")
+        srcs = np.ascontiguousarray(srcs, dtype=np.int32)
+        n = len(srcs)
+        if levels is None:
+            levels = np.empty((n, self.V), dtype=np.int32)
+        o = opts.to_c()
+        st = Stats()
+        st.struct_size = C.sizeof(Stats)
+        check(lib.xbfs_bfs_many(self._h, srcs.ctypes.data, n, _ptr(levels), C.byref(o), C.byref(st)))
+        return BfsResult(levels=levels, parents=None, depth=st.depth, reached=st.reached, edges_mc=st.edges_mc,
+                         device_ms=st.device_ms, total_ms=st.total_ms, kernel_ms=st.kernel_ms,
+                         strategies={"td_queue": st.n_td_queue, "td_scan": st.n_td_scan, "bu": st.n_bu},
+                         n_async=st.n_async)
 
     def bfs_batch(self, srcs, levels=None, words_per_vertex: int = 0, direction: Optional[str] = None,
                   alpha: float = 0.0, stream: int = 0) -> BfsResult:

@@ -68,6 +68,7 @@ constexpr int kFlushAt = kCap - kTE;
 constexpr int kFlushAtL = kCapL / 2;  // large-bin overflow goes straight to the global queue
 constexpr int kTileW = kWin / 32;   // bitmap words per dense fused-sweep sub-tile
 constexpr int kHeavyDeg = 4096;     // fused sweep: larger degrees are deferred to the heavy list
+constexpr long long kSpecEdges = 1 << 16;  // frontiers with at most this many edges claim speculatively
 
 constexpr unsigned long long kCountMask = (1ull << 31) - 1;
 
@@ -89,7 +90,6 @@ struct LevelRecDev {
 
 struct Ctl {
   GridBarrier bar;
-  int err;
   int depth;
   unsigned long long n_async;   // vertices given level+2 by bottom-up
   unsigned long long reached;   // sum of frontier sizes
@@ -136,6 +136,7 @@ struct Params {
   long long stop_level;
   int resume;
   int bu_mode;       // bottom-up neighbour probe shape (see probe_range)
+  int absent_block;  // failure-detection test hook: CTA absent_block-1 leaves at once
 };
 
 // ---------------------------------------------------------------------------
@@ -153,6 +154,7 @@ struct __align__(16) Smem {
   long long stl_bg[kCapL];
   int cnt[3];
   int strategy;
+  int spec;                     // this level's frontier is small: speculative claims
   int next_s;
   int bu_next;
   int bu_n;
@@ -383,17 +385,31 @@ struct Acc {
 };
 
 // Top-down claim of v (reached from u) for level L+1.
+// On a large frontier most edges lead to visited vertices, so a plain read of
+// the visited word filters them before the atomic; on a small one (spec) the
+// latency of each level is what counts: the claim goes straight to the atomic
+// and the vertex's CSR offsets are loaded alongside it, before it is known
+// whether this thread wins.
 template <bool PAR>
 __device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& q, Acc& acc, int v, int u,
-                                         int L, bool enq, uint32_t* fbn) {
+                                         int L, bool enq, uint32_t* fbn, bool spec) {
   const uint32_t word = (uint32_t)v >> 5, bit = 1u << (v & 31);
-  if (ld_cg_u32(p.vis + word) & bit) return;
+  long long b0 = 0, b1 = 0;
+  if (spec) {
+    b0 = ld_nc_i64(p.beg + v);
+    b1 = ld_nc_i64(p.beg + v + 1);
+  } else if (ld_cg_u32(p.vis + word) & bit) {
+    return;
+  }
   const uint32_t old = atomicOr(p.vis + word, bit);
   if (old & bit) return;
   p.levels[v] = L + 1;
   if (PAR) p.parents[v] = u;
-  const long long b0 = ld_nc_i64(p.beg + v);
-  const long long d = ld_nc_i64(p.beg + v + 1) - b0;
+  if (!spec) {
+    b0 = ld_nc_i64(p.beg + v);
+    b1 = ld_nc_i64(p.beg + v + 1);
+  }
+  const long long d = b1 - b0;
   acc.n1 += 1;
   acc.m1 += d;
   if (enq) {
@@ -441,6 +457,7 @@ template <bool PAR>
 __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
                            unsigned long long M, int L, bool enq, uint32_t* fbn) {
   if (cnt == 0 || M == 0) return;
+  const bool spec = sm.spec != 0;
   const unsigned long long G = gridDim.x, b = blockIdx.x;
   const unsigned long long lo = M * b / G, hi = M * (b + 1) / G;
   if (lo >= hi) return;
@@ -472,12 +489,65 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
       if (e < rhi) {
         const int a = smem_owner(sm.web, kTE + 1, e);
         const int v = ld_stream_i32(p.csr + sm.wbeg[a] + (long long)(e - sm.web[a]));
-        claim_td<PAR>(p, sm, q, acc, v, sm.wu[a], L, enq, fbn);
+        claim_td<PAR>(p, sm, q, acc, v, sm.wu[a], L, enq, fbn, spec);
       }
     }
     if (threadIdx.x == 0 && rhi < hi) sm.next_s = (int)(s + smem_owner(sm.web, kTE + 1, rhi));
     __syncthreads();
     s = (unsigned)sm.next_s;
+    if (enq && need_flush(sm)) flush(sm, q);
+  }
+}
+
+// Expansion of the small-degree bin (every entry has 1..small_max edges):
+// each CTA takes an equal share of the ENTRIES, so no CTA has to search the
+// queue for where its share starts. A tile of kBlock entries is loaded one
+// per thread, a block scan of their degrees gives each edge its owner, and
+// the tile's edges are expanded four per thread per pass with the CSR loads
+// issued before the claims. Degrees within the bin differ by at most
+// small_max, so shares of many entries carry similar numbers of edges.
+template <bool PAR>
+__device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
+                               unsigned long long M, int L, bool enq, uint32_t* fbn) {
+  if (cnt == 0) return;
+  const bool spec = sm.spec != 0;
+  const unsigned long long G = gridDim.x, b = blockIdx.x;
+  const unsigned i0 = (unsigned)((unsigned long long)cnt * b / G);
+  const unsigned i1 = (unsigned)((unsigned long long)cnt * (b + 1) / G);
+  for (unsigned t0 = i0; t0 < i1; t0 += kBlock) {
+    const unsigned i = t0 + threadIdx.x;
+    long long d = 0;
+    if (i < i1) {
+      const unsigned long long e0 = in.eb[i];
+      const unsigned long long e1 = (i + 1 < cnt) ? (unsigned long long)in.eb[i + 1] : M;
+      d = (long long)(e1 - e0);
+      sm.wu[threadIdx.x] = in.ids[i];
+      sm.wbeg[threadIdx.x] = in.bg[i];
+    }
+    long long total;
+    const long long ex = block_exclusive_scan<kBlock, long long>(d, sm.red, &total);
+    sm.web[threadIdx.x] = (unsigned)ex;
+    __syncthreads();
+    const int n = (int)min((unsigned)kBlock, i1 - t0);
+    const long long T = total;
+    for (long long e0 = threadIdx.x; e0 < T; e0 += 4 * kBlock) {
+      int v[4], u[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const long long e = e0 + (long long)k * kBlock;
+        v[k] = -1;
+        u[k] = 0;
+        if (e < T) {
+          const int a = smem_owner(sm.web, n, (unsigned long long)e);
+          v[k] = ld_stream_i32(p.csr + sm.wbeg[a] + (e - (long long)sm.web[a]));
+          u[k] = sm.wu[a];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (v[k] >= 0) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, enq, fbn, spec);
+    }
+    __syncthreads();
     if (enq && need_flush(sm)) flush(sm, q);
   }
 }
@@ -490,6 +560,7 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
 template <bool PAR>
 __device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc, const uint32_t* fbc, int L,
                               bool enq, uint32_t* fbn, int par) {
+  const bool spec = sm.spec != 0;
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
@@ -568,7 +639,7 @@ __device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc
         if (e < T) {
           const int a = smem_owner(sm.web, n, (unsigned long long)e);
           const int v = __ldg(p.csr + sm.wbeg[a] + (e - (long long)sm.web[a]));
-          claim_td<PAR>(p, sm, q, acc, v, sm.wu[a], L, enq, fbn);
+          claim_td<PAR>(p, sm, q, acc, v, sm.wu[a], L, enq, fbn, spec);
         }
       }
       __syncthreads();
@@ -660,6 +731,7 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= n) break;
     const int i = base + lane;
+    uint32_t word = 0xffffffffu, m1 = 0, m2 = 0;  // bitmap word of this lane's vertex, bits to set
     if (i < n) {
       const int v = list[i];
       const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
@@ -674,22 +746,41 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
         if (found < 0) probe_range<4, true, ASYNC>(p, fbc, fbn, e, e0 + 6 < e1 ? e0 + 6 : e1, found, found2);
         if (found < 0) probe_range<8, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
       }
-      const uint32_t word = (uint32_t)v >> 5, bit = 1u << (v & 31);
+      word = (uint32_t)v >> 5;
+      const uint32_t bit = 1u << (v & 31);
       if (found >= 0) {
         p.levels[v] = L + 1;
         if (PAR) p.parents[v] = found;
-        red_or_u32(p.vis + word, bit);
-        red_or_u32(fbn + word, bit);
+        m1 = bit;
         acc.n1 += 1;
         acc.m1 += e1 - e0;
       } else if (ASYNC && found2 >= 0) {
         p.levels[v] = L + 2;
         if (PAR) p.parents[v] = found2;
-        red_or_u32(p.vis + word, bit);
-        red_or_u32(fbn2 + word, bit);
+        m2 = bit;
         acc.n2 += 1;
         acc.m2 += e1 - e0;
       }
+    }
+    // The warp's 32 vertices are consecutive entries of a sorted list, so
+    // vertices sharing a bitmap word sit in adjacent lanes: OR their bits
+    // along each run of equal words and let the run's first lane publish
+    // them, one atomic per word instead of one per vertex.
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t ow = __shfl_down_sync(0xffffffffu, word, off);
+      const uint32_t o1 = __shfl_down_sync(0xffffffffu, m1, off);
+      const uint32_t o2 = __shfl_down_sync(0xffffffffu, m2, off);
+      if (lane + off < 32 && ow == word) {
+        m1 |= o1;
+        m2 |= o2;
+      }
+    }
+    const uint32_t pw = __shfl_up_sync(0xffffffffu, word, 1);
+    if (i < n && (lane == 0 || pw != word)) {
+      if (m1 | m2) red_or_u32(p.vis + word, m1 | m2);
+      if (m1) red_or_u32(fbn + word, m1);
+      if (ASYNC && m2) red_or_u32(fbn2 + word, m2);
     }
   }
 }
@@ -727,6 +818,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   Ctl* ctl = p.ctl;
+  if (p.absent_block > 0 && (int)blockIdx.x == p.absent_block - 1) return;  // test hook: never arrives
   if (threadIdx.x < 3) sm.cnt[threadIdx.x] = 0;
   __syncthreads();
 
@@ -777,7 +869,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       break;
     }
     if (L >= p.max_levels) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctl->err, 0, (int)XBFS_ERR_INTERNAL);
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctl->bar.err, 0, (int)XBFS_ERR_INTERNAL);
       break;
     }
     FDesc* F0 = &ctl->fd[L & 3];
@@ -794,6 +886,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
 #pragma unroll
       for (int b2 = 0; b2 < 3; ++b2) sm.bins[b2] = ld_cg_u64(&F0->bin[b2]);
       sm.pend_next = pn;
+      sm.spec = m_f <= kSpecEdges ? 1 : 0;
       int s = -1;
       if (n_f > 0) {
         vis_n += n_f;
@@ -889,16 +982,18 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       for (int b2 = 0; b2 < 3; ++b2) qo.b[b2] = p.q[par ^ 1][b2];
       qo.ctr = F1->bin;
       if (q_valid) {
-        for (int bin = 2; bin >= 0; --bin) {
+        for (int bin = 2; bin >= 1; --bin) {
           const unsigned long long pk = sm.bins[bin];
           gather_bin<PAR>(p, sm, qo, acc, p.q[par][bin], (unsigned)(pk & kCountMask), pk >> 31, (int)L, enq, fbn);
         }
+        const unsigned long long pk0 = sm.bins[0];
+        gather_entries<PAR>(p, sm, qo, acc, p.q[par][0], (unsigned)(pk0 & kCountMask), pk0 >> 31, (int)L, enq, fbn);
       } else {
         expand_bitmap<PAR>(p, sm, qo, acc, fbc, (int)L, enq, fbn, par);
       }
       if (enq) flush(sm, qo);
       publish_acc(sm, acc, F1, nullptr);
-      if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+      if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       if (!q_valid) {
         // heavy vertices deferred by the fused sweep: expand them grid-wide
         // (the list is complete only after the barrier; usually it is empty)
@@ -907,7 +1002,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
           gather_bin<PAR>(p, sm, qo, acc, p.heavy, (unsigned)(hk & kCountMask), hk >> 31, (int)L, enq, fbn);
           if (enq) flush(sm, qo);
           publish_acc(sm, acc, F1, nullptr);
-          if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+          if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
         }
       }
       q_valid = enq;
@@ -917,14 +1012,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       if (!b_valid) {
         scatter_queue_to_bitmap(p, par, *F0, fbc);
         dirty |= 1u << (L & 3);
-        if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+        if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       }
       if (p.async_bu)
         bottom_up<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
       else
         bottom_up<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
       publish_acc(sm, acc, F1, F2);
-      if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+      if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       q_valid = false;
       b_valid = true;
       dirty |= 1u << ((L + 1) & 3);
@@ -1053,7 +1148,9 @@ static xbfs_status setup_params(Graph* g, const xbfs_opts& o, int* d_levels, int
   p.medium_max = o.medium_max;
   p.beamer_alpha = o.beamer_alpha > 0 ? o.beamer_alpha : 14.f;
   p.beamer_beta = o.beamer_beta > 0 ? o.beamer_beta : 24.f;
-  p.timeout_ns = 10ull * 1000 * 1000 * 1000;
+  p.timeout_ns = o.wait_timeout_us > 0 ? (unsigned long long)o.wait_timeout_us * 1000ull
+                                        : 10ull * 1000 * 1000 * 1000;
+  p.absent_block = o.test_absent_block;
   p.max_levels = g->V + 2;
   extern const float* mlp_device_weights(int device);
   p.mlp = mlp_device_weights(g->device);
@@ -1073,7 +1170,7 @@ static xbfs_status setup_params(Graph* g, const xbfs_opts& o, int* d_levels, int
   w.grid = grid;
   w.block = kBlock;
   p.rs = w.rs.as<ResumeState>();
-  p.bu_mode = o.reserved[0];
+  p.bu_mode = o.bu_probe;
   p.stop_level = LLONG_MAX;
   p.resume = 0;
   *kfn_out = kfn;
@@ -1171,8 +1268,8 @@ xbfs_status bfs_single(Graph* g, int32_t src, int32_t* levels, int32_t* parents,
   if (parents && !par_dev)
     XBFS_CUDA_TRY(cudaMemcpyAsync(parents, d_parents, (size_t)g->V * 4, cudaMemcpyDeviceToHost, s));
   XBFS_CUDA_TRY(cudaStreamSynchronize(s));
-  if (hctl.err != 0)
-    return set_error((xbfs_status)hctl.err, "traversal kernel reported %s", xbfs_strerror(hctl.err));
+  if (hctl.bar.err != 0)
+    return set_error((xbfs_status)hctl.bar.err, "traversal kernel reported %s", xbfs_strerror(hctl.bar.err));
   w.last_levels = hctl.depth;
   float ms = 0, kms = 0;
   XBFS_CUDA_TRY(cudaEventElapsedTime(&ms, w.ev0, w.ev1));
@@ -1204,6 +1301,131 @@ xbfs_status bfs_single(Graph* g, int32_t src, int32_t* levels, int32_t* parents,
     stats->n_td_scan = hctl.strat_count[1];
     stats->n_bu = hctl.strat_count[2];
     stats->n_async = (int32_t)hctl.n_async;
+    stats->total_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  }
+  return XBFS_OK;
+}
+
+// n single-source traversals in one call, pipelined: while traversal i runs
+// on the graph's stream, the level array of traversal i-1 is copied out on a
+// second stream, so a host output costs max(kernel, copy) per source instead
+// of their sum. Two device level buffers alternate; traversal i+2 waits for
+// the copy that frees its buffer. With device outputs the kernels write the
+// rows directly and nothing is copied.
+xbfs_status bfs_many(Graph* g, const int32_t* srcs, int32_t n, int32_t* levels, const xbfs_opts* uopts,
+                     xbfs_stats* stats) {
+  const auto t_start = std::chrono::steady_clock::now();
+  xbfs_opts o;
+  xbfs_opts_init(&o);
+  if (uopts) {
+    if (uopts->struct_size != (int32_t)sizeof(xbfs_opts))
+      return set_error(XBFS_ERR_INVALID_ARG, "xbfs_opts.struct_size = %d, expected %zu (call xbfs_opts_init)",
+                       uopts->struct_size, sizeof(xbfs_opts));
+    o = *uopts;
+  }
+  if (!g || !srcs || !levels || n <= 0) return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
+  for (int i = 0; i < n; ++i)
+    if (srcs[i] < 0 || (int64_t)srcs[i] >= g->V)
+      return set_error(XBFS_ERR_INVALID_ARG, "source %d (%d) out of range [0, %lld)", i, srcs[i], (long long)g->V);
+  if (g->E >= (1ll << 32))
+    return set_error(XBFS_ERR_UNSUPPORTED, "single-source path needs E < 2^32 (E = %lld)", (long long)g->E);
+  if (o.padding != 1) return set_error(XBFS_ERR_INVALID_ARG, "padding = %d: only 1 is supported", o.padding);
+  if (o.policy == XBFS_POLICY_FORCED && (!o.forced || o.n_forced <= 0))
+    return set_error(XBFS_ERR_INVALID_ARG, "forced policy needs a non-empty forced[] array");
+  if (o.policy < 0 || o.policy > 3) return set_error(XBFS_ERR_INVALID_ARG, "bad policy %d", o.policy);
+  if (o.small_max <= 0) o.small_max = 32;
+  if (o.medium_max < o.small_max) o.medium_max = o.small_max;
+  if (!(o.alpha > 0)) o.alpha = 0.1f;
+
+  DeviceGuard dg(g->device);
+  xbfs_status st = ensure_workspace(g, o.small_max, o.medium_max);
+  if (st) return st;
+  SsWorkspace& w = g->ss;
+  cudaStream_t s = o.stream ? (cudaStream_t)o.stream : g->stream;
+  const bool dev_out = is_device_pointer(levels);
+  const size_t row = (size_t)g->V;
+  if (!dev_out) {
+    if ((st = w.levels_tmp.ensure(row * 4)) || (st = w.levels_tmp2.ensure(row * 4))) return st;
+    if (!w.copy_stream) XBFS_CUDA_TRY(cudaStreamCreateWithFlags(&w.copy_stream, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      if (!w.ev_done[b]) XBFS_CUDA_TRY(cudaEventCreateWithFlags(&w.ev_done[b], cudaEventDisableTiming));
+      if (!w.ev_copied[b]) XBFS_CUDA_TRY(cudaEventCreateWithFlags(&w.ev_copied[b], cudaEventDisableTiming));
+    }
+  }
+  if ((st = w.ctl_log.ensure(sizeof(Ctl) * (size_t)n))) return st;
+  if (o.policy == XBFS_POLICY_FORCED) {
+    if (o.n_forced > w.forced_cap) {
+      if ((st = w.forced.ensure((size_t)o.n_forced))) return st;
+      w.forced_cap = o.n_forced;
+    }
+    XBFS_CUDA_TRY(cudaMemcpyAsync(w.forced.p, o.forced, (size_t)o.n_forced, cudaMemcpyHostToDevice, s));
+  }
+  int* dbuf[2] = {w.levels_tmp.as<int>(), w.levels_tmp2.as<int>()};
+  Params p;
+  const void* kfn = nullptr;
+  size_t smem = 0;
+  int grid = 0;
+  if ((st = setup_params(g, o, dev_out ? levels : dbuf[0], nullptr, p, &kfn, &smem, &grid))) return st;
+
+  XBFS_CUDA_TRY(cudaEventRecord(w.ev0, s));
+  auto copy_out = [&](int i) -> xbfs_status {
+    const int b = i & 1;
+    XBFS_CUDA_TRY(cudaStreamWaitEvent(w.copy_stream, w.ev_done[b], 0));
+    XBFS_CUDA_TRY(cudaMemcpyAsync(levels + (size_t)i * row, dbuf[b], row * 4, cudaMemcpyDeviceToHost,
+                                  w.copy_stream));
+    XBFS_CUDA_TRY(cudaEventRecord(w.ev_copied[b], w.copy_stream));
+    return XBFS_OK;
+  };
+  for (int i = 0; i < n; ++i) {
+    const int b = i & 1;
+    if (dev_out) {
+      p.levels = levels + (size_t)i * row;
+    } else {
+      p.levels = dbuf[b];
+      if (i >= 2) XBFS_CUDA_TRY(cudaStreamWaitEvent(s, w.ev_copied[b], 0));  // buffer copied out
+    }
+    if ((st = init_state(g, p, srcs[i], false, s))) return st;
+    void* args[] = {&p};
+    XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, smem, s));
+    XBFS_CUDA_TRY(cudaMemcpyAsync(w.ctl_log.as<Ctl>() + i, p.ctl, sizeof(Ctl), cudaMemcpyDeviceToDevice, s));
+    if (!dev_out) {
+      XBFS_CUDA_TRY(cudaEventRecord(w.ev_done[b], s));
+      // the copy of the previous traversal is issued after this launch, so
+      // a pageable destination (whose copy blocks the host) still overlaps
+      if (i > 0 && (st = copy_out(i - 1))) return st;
+    }
+  }
+  if (!dev_out && (st = copy_out(n - 1))) return st;
+  XBFS_CUDA_TRY(cudaEventRecord(w.ev1, s));
+  std::vector<Ctl> hctl((size_t)n);
+  XBFS_CUDA_TRY(cudaMemcpyAsync(hctl.data(), w.ctl_log.p, sizeof(Ctl) * (size_t)n, cudaMemcpyDeviceToHost, s));
+  XBFS_CUDA_TRY(cudaStreamSynchronize(s));
+  if (!dev_out) XBFS_CUDA_TRY(cudaStreamSynchronize(w.copy_stream));
+  long long reached = 0, msum = 0, n_async = 0;
+  int depth = 0, sc[3] = {0, 0, 0};
+  for (int i = 0; i < n; ++i) {
+    if (hctl[i].bar.err != 0)
+      return set_error((xbfs_status)hctl[i].bar.err, "traversal %d reported %s", i, xbfs_strerror(hctl[i].bar.err));
+    reached += (long long)hctl[i].reached;
+    msum += (long long)hctl[i].msum;
+    n_async += (long long)hctl[i].n_async;
+    depth = std::max(depth, hctl[i].depth);
+    for (int k = 0; k < 3; ++k) sc[k] += hctl[i].strat_count[k];
+  }
+  if (stats) {
+    float ms = 0;
+    XBFS_CUDA_TRY(cudaEventElapsedTime(&ms, w.ev0, w.ev1));
+    stats->struct_size = (int32_t)sizeof(xbfs_stats);
+    stats->depth = depth;
+    stats->reached = reached;
+    stats->edges_mc = msum / 2;
+    stats->device_ms = ms;
+    stats->kernel_ms = 0.0;
+    stats->n_td_queue = sc[0];
+    stats->n_td_scan = sc[1];
+    stats->n_bu = sc[2];
+    stats->n_async = (int32_t)n_async;
     stats->total_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
   }
@@ -1242,31 +1464,51 @@ xbfs_status level_costs(Graph* g, int32_t src, int32_t follow, int32_t cap, floa
   size_t smem = 0;
   int grid = 0;
   if ((st = setup_params(g, o, w.levels_tmp.as<int>(), nullptr, p, &kfn, &smem, &grid))) return st;
-  // snapshot layout: levels | bitmaps | queues (2 parities x 3 bins) | ctl | resume state
+  // A snapshot holds the state a level starts from: levels, the five
+  // bitmaps, the live part of the frontier queue (parity of the level, the
+  // entries its descriptor counts), the control block and the resume state.
   struct Piece { void* p; size_t n; };
-  std::vector<Piece> pieces;
-  pieces.push_back({w.levels_tmp.p, (size_t)g->V * 4});
-  pieces.push_back({w.bits.p, w.nwords * 4 * 5});
-  for (int par = 0; par < 2; ++par)
+  struct Snap { DevBuf* buf; std::vector<Piece> pieces; };
+  auto live_pieces = [&](long long level, const FDesc& f) {
+    std::vector<Piece> v;
+    v.push_back({w.levels_tmp.p, (size_t)g->V * 4});
+    v.push_back({w.bits.p, w.nwords * 4 * 5});
+    const int par = (int)(level & 1);
     for (int b = 0; b < 3; ++b) {
-      pieces.push_back({w.qids[par][b].p, w.qcap[b] * 4});
-      pieces.push_back({w.qeb[par][b].p, w.qcap[b] * 4});
-      pieces.push_back({w.qbg[par][b].p, w.qcap[b] * 8});
+      const size_t cnt = (size_t)(f.bin[b] & kCountMask);
+      if (!cnt) continue;
+      v.push_back({w.qids[par][b].p, cnt * 4});
+      v.push_back({w.qeb[par][b].p, cnt * 4});
+      v.push_back({w.qbg[par][b].p, cnt * 8});
     }
-  pieces.push_back({w.ctl.p, sizeof(Ctl)});
-  pieces.push_back({w.rs.p, sizeof(ResumeState)});
+    v.push_back({w.ctl.p, sizeof(Ctl)});
+    v.push_back({w.rs.p, sizeof(ResumeState)});
+    return v;
+  };
   size_t total = 0;
-  for (auto& pc : pieces) total += (pc.n + 255) & ~(size_t)255;
+  {
+    FDesc full;
+    memset(&full, 0, sizeof(full));
+    for (int b = 0; b < 3; ++b) full.bin[b] = (unsigned long long)w.qcap[b];
+    for (auto& pc : live_pieces(0, full)) total += (pc.n + 255) & ~(size_t)255;
+  }
   if ((st = w.snap.ensure(total))) return st;
-  auto copy_all = [&](bool save) -> xbfs_status {
+  if ((st = w.snap2.ensure(total))) return st;
+  Snap s1{&w.snap, {}}, s2{&w.snap2, {}};
+  auto copy_snap = [&](Snap& sn, bool save) -> xbfs_status {
     size_t off = 0;
-    for (auto& pc : pieces) {
-      char* sp = w.snap.as<char>() + off;
+    for (auto& pc : sn.pieces) {
+      char* sp = sn.buf->as<char>() + off;
       XBFS_CUDA_TRY(cudaMemcpyAsync(save ? sp : pc.p, save ? pc.p : sp, pc.n, cudaMemcpyDeviceToDevice, s));
       off += (pc.n + 255) & ~(size_t)255;
     }
     return XBFS_OK;
   };
+  auto save_snap = [&](Snap& sn, long long level, const FDesc& f) -> xbfs_status {
+    sn.pieces = live_pieces(level, f);
+    return copy_snap(sn, true);
+  };
+  auto copy_all = [&](bool save) -> xbfs_status { return copy_snap(s1, save); };
   auto run_level = [&](int L, int strategy, int policy, LevelRecDev* rec) -> xbfs_status {
     forced[L] = (signed char)strategy;
     XBFS_CUDA_TRY(cudaMemcpyAsync(w.forced.p, forced.data(), (size_t)L + 1, cudaMemcpyHostToDevice, s));
@@ -1279,7 +1521,7 @@ xbfs_status level_costs(Graph* g, int32_t src, int32_t follow, int32_t cap, floa
     XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, smem, s));
     XBFS_CUDA_TRY(cudaMemcpyAsync(rec, p.hist + L, sizeof(LevelRecDev), cudaMemcpyDeviceToHost, s));
     int err = 0;
-    XBFS_CUDA_TRY(cudaMemcpyAsync(&err, &p.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    XBFS_CUDA_TRY(cudaMemcpyAsync(&err, &p.ctl->bar.err, sizeof(int), cudaMemcpyDeviceToHost, s));
     XBFS_CUDA_TRY(cudaStreamSynchronize(s));
     if (err) return set_error((xbfs_status)err, "stepped traversal reported %s", xbfs_strerror(err));
     return XBFS_OK;
@@ -1292,12 +1534,33 @@ xbfs_status level_costs(Graph* g, int32_t src, int32_t follow, int32_t cap, floa
     XBFS_CUDA_TRY(cudaMemcpyAsync(&f, &p.ctl->fd[L & 3], sizeof(FDesc), cudaMemcpyDeviceToHost, s));
     XBFS_CUDA_TRY(cudaStreamSynchronize(s));
     if (f.n == 0) break;
-    if ((st = copy_all(true))) return st;
+    if ((st = save_snap(s1, L, f))) return st;
     LevelRecDev rec[3];
     for (int k = 0; k < 3; ++k) {
       if (k > 0 && (st = copy_all(false))) return st;
       if ((st = run_level(L, k, XBFS_POLICY_FORCED, &rec[k]))) return st;
       costs[L * 3 + k] = (rec[k].t1 > rec[k].t0) ? (float)((rec[k].t1 - rec[k].t0) * 1e-3) : 0.f;
+      // one level of lookahead: a strategy also fixes the form of the next
+      // frontier (queue or bitmap) and with it the next level's input cost,
+      // so the cost of k is this level plus the cheapest next level (each
+      // strategy tried from the state k left behind)
+      if (L + 1 < cap) {
+        FDesc nf;
+        XBFS_CUDA_TRY(cudaMemcpyAsync(&nf, &p.ctl->fd[(L + 1) & 3], sizeof(FDesc), cudaMemcpyDeviceToHost, s));
+        XBFS_CUDA_TRY(cudaStreamSynchronize(s));
+        if (nf.n != 0) {
+          if ((st = save_snap(s2, L + 1, nf))) return st;
+          float best = 0.f;
+          for (int j = 0; j < 3; ++j) {
+            if (j > 0 && (st = copy_snap(s2, false))) return st;
+            LevelRecDev r2;
+            if ((st = run_level(L + 1, j, XBFS_POLICY_FORCED, &r2))) return st;
+            const float t2 = (r2.t1 > r2.t0) ? (float)((r2.t1 - r2.t0) * 1e-3) : 0.f;
+            if (j == 0 || t2 < best) best = t2;
+          }
+          costs[L * 3 + k] += best;
+        }
+      }
     }
     int choice = 0;
     if (follow == 1) {
@@ -1509,7 +1772,7 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
   if (o.policy == XBFS_POLICY_MLP && !p.mlp) p.policy = XBFS_POLICY_HEURISTIC;
   p.allow_bu = g->symmetric ? 1 : 0;
   p.rs = (ResumeState*)(base + o_rs);
-  p.bu_mode = o.reserved[0];
+  p.bu_mode = o.bu_probe;
   p.stop_level = LLONG_MAX;
   p.resume = 0;
   const bool par_on = parents != nullptr;
@@ -1533,8 +1796,8 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
   Ctl hctl;
   XBFS_CUDA_TRY(cudaMemcpyAsync(&hctl, p.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   XBFS_CUDA_TRY(cudaStreamSynchronize(s));
-  if (hctl.err != 0)
-    return set_error((xbfs_status)hctl.err, "traversal kernel reported %s", xbfs_strerror(hctl.err));
+  if (hctl.bar.err != 0)
+    return set_error((xbfs_status)hctl.bar.err, "traversal kernel reported %s", xbfs_strerror(hctl.bar.err));
   if (stats) {
     stats->struct_size = (int32_t)sizeof(xbfs_stats);
     stats->depth = hctl.depth;
@@ -1561,6 +1824,11 @@ extern "C" {
 xbfs_status xbfs_bfs(xbfs_graph* gh, int32_t src, int32_t* levels, int32_t* parents, const xbfs_opts* opts,
                      xbfs_stats* stats) {
   return bfs_single((Graph*)gh, src, levels, parents, opts, stats);
+}
+
+xbfs_status xbfs_bfs_many(xbfs_graph* gh, const int32_t* srcs, int32_t n, int32_t* levels, const xbfs_opts* opts,
+                          xbfs_stats* stats) {
+  return bfs_many((Graph*)gh, srcs, n, levels, opts, stats);
 }
 
 xbfs_status xbfs_bfs_noalloc(xbfs_graph* gh, int32_t src, int32_t* levels, int32_t* parents,

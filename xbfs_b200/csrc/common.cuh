@@ -87,21 +87,24 @@ __device__ __forceinline__ long long ld_nc_i64(const long long* p) {
 // false, so the launch ends and the host reads a status instead of the GPU
 // hanging. Any block that sees a non-zero error word also leaves.
 // ---------------------------------------------------------------------------
-struct GridBarrier {
+struct __align__(8) GridBarrier {
   uint32_t count;  // arrivals since launch (zeroed before the launch)
-  uint32_t pad;
+  int32_t err;     // launch status (xbfs_status), 0 = fine; shares count's 8 bytes
 };
 
-// Count-up barrier: the k-th barrier of a launch completes when `count`
-// reaches k * nblocks. One release-add per CTA, no reset and no generation
-// flip on the critical path; `epoch` is the CTA's own count of barriers
-// passed (identical in all CTAs). 2^32 arrivals allow > 10^7 barriers at
-// 296 CTAs.
 __device__ __forceinline__ void red_add_release_u32(uint32_t* p, uint32_t v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ bool grid_sync(GridBarrier* bar, uint32_t nblocks, uint32_t& epoch, int* err,
+// Count-up barrier: the k-th barrier of a launch completes when `count`
+// reaches k * nblocks. One release-add per CTA (the block barrier before it
+// makes the whole CTA's writes part of the release), no reset and no
+// generation flip on the critical path; `epoch` is the CTA's own count of
+// barriers passed (identical in all CTAs). Each poll is one 8-byte acquire
+// load that returns the arrival count and the error word together, so the
+// barrier costs one release and the polls, with no separate fence or status
+// read. 2^32 arrivals allow > 10^7 barriers at 296 CTAs.
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar, uint32_t nblocks, uint32_t& epoch,
                                           unsigned long long timeout_ns) {
   __shared__ int s_ok;
   __syncthreads();
@@ -109,25 +112,27 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar, uint32_t nblocks, ui
   if (threadIdx.x == 0) {
     int ok = 1;
     const uint32_t target = epoch * nblocks;
-    __threadfence();
     red_add_release_u32(&bar->count, 1u);
     uint32_t spins = 0;
     unsigned long long t0 = 0;
-    while ((int32_t)(ld_acquire_u32(&bar->count) - target) < 0) {
+    for (;;) {
+      const unsigned long long w = ld_acquire_u64(reinterpret_cast<const unsigned long long*>(bar));
+      if ((int32_t)(w >> 32) != 0) {
+        ok = 0;
+        break;
+      }
+      if ((int32_t)((uint32_t)w - target) >= 0) break;
       ++spins;
       if (spins > 2048) __nanosleep(32);
       if ((spins & 1023u) == 0) {
         if (t0 == 0) t0 = globaltimer_ns();
-        if (ld_acquire_i32(err) != 0) { ok = 0; break; }
         if (globaltimer_ns() - t0 > timeout_ns) {
-          atomicCAS(err, 0, (int)XBFS_ERR_DEVICE_TIMEOUT);
+          atomicCAS(&bar->err, 0, (int)XBFS_ERR_DEVICE_TIMEOUT);
           ok = 0;
           break;
         }
       }
     }
-    __threadfence();
-    if (ok && ld_acquire_i32(err) != 0) ok = 0;
     s_ok = ok;
   }
   __syncthreads();

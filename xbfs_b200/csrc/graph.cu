@@ -70,6 +70,11 @@ Graph::~Graph() {
   if (ss.ev0) cudaEventDestroy(ss.ev0);
   if (ss.ev1) cudaEventDestroy(ss.ev1);
   if (ss.evk0) cudaEventDestroy(ss.evk0);
+  for (int i = 0; i < 2; ++i) {
+    if (ss.ev_done[i]) cudaEventDestroy(ss.ev_done[i]);
+    if (ss.ev_copied[i]) cudaEventDestroy(ss.ev_copied[i]);
+  }
+  if (ss.copy_stream) cudaStreamDestroy(ss.copy_stream);
   if (stream) cudaStreamDestroy(stream);
 }
 

@@ -59,11 +59,18 @@ struct SsWorkspace {
   DevBuf ctl;              // control block
   DevBuf rs;               // loop state of a stepped traversal
   DevBuf snap;             // snapshot of the whole traversal state (stepped mode)
+  DevBuf snap2;            // second snapshot: the state one strategy left after a level
   DevBuf hist;             // per-level records
   int hist_cap = 0;
   DevBuf forced;           // int8 per-level strategies
   int forced_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr;
+  // pipelined traversals (xbfs_bfs_many): a second level buffer, the stream
+  // that copies finished level arrays out, and the events between the two
+  DevBuf levels_tmp2;
+  DevBuf ctl_log;          // Ctl of every traversal of one call
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_done[2] = {nullptr, nullptr}, ev_copied[2] = {nullptr, nullptr};
   int grid = 0, block = 0;
   int last_levels = 0;
   std::vector<xbfs_level_trace> trace;

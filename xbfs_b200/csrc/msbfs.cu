@@ -37,7 +37,6 @@ constexpr unsigned long long kCountMask = (1ull << 31) - 1;
 
 struct Ctl {
   GridBarrier bar;
-  int err;
   int depth;
   unsigned long long q[3];        // packed (edges << 31) | count, frontier queue ring
   unsigned int tcount[2];         // touched-list length by level parity
@@ -293,7 +292,7 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
   long long L = 0;
   for (;; ++L) {
     if (L >= p.max_levels) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctl->err, 0, (int)XBFS_ERR_INTERNAL);
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctl->bar.err, 0, (int)XBFS_ERR_INTERNAL);
       break;
     }
     const int qs = (int)(L % 3), qn = (int)((L + 1) % 3), qo = (int)((L + 2) % 3);
@@ -306,7 +305,7 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
         if (L > 0) m_done_total += (long long)ld_cg_u64(&ctl->m_done[(L - 1) % 3]);
         const long long m_u = p.m_active - m_done_total;
         if (L + 1 >= p.row_max) {
-          atomicCAS(&ctl->err, 0, (int)XBFS_ERR_LEVEL_OVERFLOW);
+          atomicCAS(&ctl->bar.err, 0, (int)XBFS_ERR_LEVEL_OVERFLOW);
           d = -1;
         } else if (p.force == 0 || !p.allow_bu) {
           d = 0;
@@ -343,7 +342,7 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
     if (D == 0) {
       // ---------------- top-down: push along the edges of the frontier queue
       ms_gather<W, RowT, false>(p, sm, qin, qeb_in, cnt, mf, Fc, &ctl->tcount[L & 1]);
-      if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+      if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       ms_merge<W, RowT>(p, L, Fn, qout, qeb_out, qctr, m_done, n_done);
     } else {
       // ---------------- bottom-up: light vertices search their neighbours
@@ -425,12 +424,12 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
         warp_enqueue(qout, qeb_out, qctr, have && deg > 0, v, deg);
         warp_enqueue(p.hq_ids, p.hq_eb, hctr, heavy, v, deg);
       }
-      if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+      if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       const unsigned long long hk = ld_cg_u64(hctr);
       if ((hk & kCountMask) != 0) {
         ms_gather<W, RowT, true>(p, sm, p.hq_ids, p.hq_eb, (unsigned)(hk & kCountMask), hk >> 31, Fc,
                                  &ctl->tcount[L & 1]);
-        if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+        if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
         ms_merge<W, RowT>(p, L, Fn, qout, qeb_out, qctr, m_done, n_done);
       }
     }
@@ -443,7 +442,7 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
         if (nd) atomicAdd(&ctl->n_done[L % 3], (unsigned long long)nd);
       }
     }
-    if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+    if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
     // retire frontier L: clear its F entries (nobody reads them any more)
     {
       unsigned long long* Fr = p.F[L & 1];
@@ -456,7 +455,7 @@ __global__ void __launch_bounds__(kBlock, (W >= 4 ? 1 : 2)) k_msbfs(Params<W, Ro
     // sources of degree 0 are never queued and keep their F bits; no vertex has
     // them as a neighbour (bottom-up runs on symmetric graphs only), so they are
     // never read again
-    if (!grid_sync(&ctl->bar, nb, epoch, &ctl->err, p.timeout_ns)) break;
+    if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->depth = (int)L;
 }
@@ -632,7 +631,7 @@ static xbfs_status run_pass(Graph* g, const int32_t* srcs, int n, int* d_out, si
   ms::Ctl hc;
   XBFS_CUDA_TRY(cudaMemcpyAsync(&hc, p.ctl, sizeof(hc), cudaMemcpyDeviceToHost, s));
   XBFS_CUDA_TRY(cudaStreamSynchronize(s));
-  if (hc.err) return set_error((xbfs_status)hc.err, "batched traversal kernel reported %s", xbfs_strerror(hc.err));
+  if (hc.bar.err) return set_error((xbfs_status)hc.bar.err, "batched traversal kernel reported %s", xbfs_strerror(hc.bar.err));
   *depth = std::max(*depth, hc.depth);
   strat[0] += hc.strat_count[0];
   strat[1] += hc.strat_count[1];
