@@ -61,12 +61,17 @@ namespace xbfs {
 constexpr int kBlock = 512;         // threads per CTA of the traversal kernel
 constexpr int kK = 2;               // edges per thread per gather round
 constexpr int kTE = kBlock * kK;    // edges per gather round
-constexpr int kWin = 2048;          // shared window / tile list capacity
-constexpr int kCap = 2048;          // staging capacity, small and medium bins
+// Shared memory is kept near 54 KB per CTA on purpose: two CTAs per SM then
+// leave about 140 KB of the SM's 256 KB unified L1/shared storage to L1,
+// which caches the frontier-bitmap words and CSR offsets that bottom-up
+// probes read at random (doubling the staging areas cost ~30% on the
+// bottom-up level of R-MAT scale 23 through the smaller L1).
+constexpr int kWin = kTE;           // shared window / tile list capacity
+constexpr int kCap = 1024;          // staging capacity, small and medium bins
 constexpr int kCapL = 256;          // staging capacity, large bin
-constexpr int kFlushAt = kCap - kTE;
+constexpr int kFlushAt = kCap - kTE;  // a round adds at most kTE winners: flush before each
 constexpr int kFlushAtL = kCapL / 2;  // large-bin overflow goes straight to the global queue
-constexpr int kTileW = kWin / 32;   // bitmap words per dense fused-sweep sub-tile
+static_assert(kFlushAt >= 0, "a gather round must fit the staging area");
 constexpr int kHeavyDeg = 4096;     // fused sweep: larger degrees are deferred to the heavy list
 constexpr long long kSpecEdges = 1 << 16;  // frontiers with at most this many edges claim speculatively
 
@@ -139,6 +144,37 @@ struct Params {
   int absent_block;  // failure-detection test hook: CTA absent_block-1 leaves at once
 };
 
+__device__ __forceinline__ int bin_of(long long d, int small_max, int medium_max) {
+  return d <= small_max ? 0 : (d <= medium_max ? 1 : 2);
+}
+
+// ---------------------------------------------------------------------------
+// Strategy policy (computed identically by thread 0 of every CTA).
+// ---------------------------------------------------------------------------
+struct PolicyState {
+  // reference heuristic state (bfs_adaptiveFQ_wb_async.cuh:946-1078)
+  long long count_prev;
+  int is_change;
+  long long td_adaptive;
+  long long hub_before;
+  long long hub_after;
+  int tag_prev;  // 0: scan-free / last-phase TD, 1: second-phase TD, -1: BU
+  // Beamer
+  int bu_dir;
+  // features
+  long long n_prev;
+  int prev_strategy;
+};
+
+// Per-CTA loop state owned by thread 0 (in shared memory).
+struct LoopState {
+  PolicyState ps;
+  long long vis_n, vis_m;  // sums over frontiers <= L
+  // statistics of the whole traversal (used by block 0)
+  unsigned long long st_reached, st_msum, st_async;
+  int st_strat[3];
+};
+
 // ---------------------------------------------------------------------------
 // Shared memory layout of the traversal kernel (dynamic).
 // ---------------------------------------------------------------------------
@@ -165,28 +201,7 @@ struct __align__(16) Smem {
   long long red[kBlock / 32 + 1];
   long long red4[4 * (kBlock / 32)];
   float mlp_h[2][32];
-};
-
-__device__ __forceinline__ int bin_of(long long d, int small_max, int medium_max) {
-  return d <= small_max ? 0 : (d <= medium_max ? 1 : 2);
-}
-
-// ---------------------------------------------------------------------------
-// Strategy policy (computed identically by thread 0 of every CTA).
-// ---------------------------------------------------------------------------
-struct PolicyState {
-  // reference heuristic state (bfs_adaptiveFQ_wb_async.cuh:946-1078)
-  long long count_prev;
-  int is_change;
-  long long td_adaptive;
-  long long hub_before;
-  long long hub_after;
-  int tag_prev;  // 0: scan-free / last-phase TD, 1: second-phase TD, -1: BU
-  // Beamer
-  int bu_dir;
-  // features
-  long long n_prev;
-  int prev_strategy;
+  LoopState ls;
 };
 
 // Loop state carried across launches in stepped mode (xbfs_level_costs): a
@@ -503,8 +518,8 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
 // each CTA takes an equal share of the ENTRIES, so no CTA has to search the
 // queue for where its share starts. A tile of kBlock entries is loaded one
 // per thread, a block scan of their degrees gives each edge its owner, and
-// the tile's edges are expanded four per thread per pass with the CSR loads
-// issued before the claims. Degrees within the bin differ by at most
+// the tile's edges are expanded in rounds of kTE with the CSR loads issued
+// before the claims. Degrees within the bin differ by at most
 // small_max, so shares of many entries carry similar numbers of edges.
 template <bool PAR>
 __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
@@ -530,11 +545,13 @@ __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& ac
     __syncthreads();
     const int n = (int)min((unsigned)kBlock, i1 - t0);
     const long long T = total;
-    for (long long e0 = threadIdx.x; e0 < T; e0 += 4 * kBlock) {
-      int v[4], u[4];
+    // rounds of kTE edges (kK per thread, loads issued before the claims),
+    // so one round's winners always fit the staging area
+    for (long long r = 0; r < T; r += kTE) {
+      int v[kK], u[kK];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const long long e = e0 + (long long)k * kBlock;
+      for (int k = 0; k < kK; ++k) {
+        const long long e = r + threadIdx.x + (long long)k * kBlock;
         v[k] = -1;
         u[k] = 0;
         if (e < T) {
@@ -544,11 +561,12 @@ __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& ac
         }
       }
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
+      for (int k = 0; k < kK; ++k)
         if (v[k] >= 0) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, enq, fbn, spec);
+      __syncthreads();
+      if (enq && need_flush(sm)) flush(sm, q);
     }
     __syncthreads();
-    if (enq && need_flush(sm)) flush(sm, q);
   }
 }
 
@@ -565,39 +583,34 @@ __device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc
   const long long G = gridDim.x, b = blockIdx.x;
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
   unsigned long long* hctr = &p.ctl->heavy[par];
-  // A tile is kBlock words (one per thread) when its set bits fit the shared
-  // window (the common, sparse case); a denser tile is cut into sub-tiles of
-  // kTileW words, which always fit.
+  // A tile is kBlock words, one per thread. Its set bits are numbered by a
+  // block scan of the words' popcounts and taken kWin at a time (one pass
+  // for a sparse tile, ceil(bits / kWin) passes for a dense one).
   for (long long wt = w0; wt < w1; wt += kBlock) {
     uint32_t tbits = 0;
-    {
-      const long long w = wt + threadIdx.x;
-      if (w < w1) tbits = ld_cg_u32(fbc + w);
-    }
+    const long long w = wt + threadIdx.x;
+    if (w < w1) tbits = ld_cg_u32(fbc + w);
     const int tcount = __syncthreads_count(tbits != 0);
     if (tcount == 0) continue;
-    long long tsum = block_sum<kBlock, long long>((long long)__popc(tbits), sm.red);
-    const bool whole = tsum <= kWin;
-    const long long wend = (wt + kBlock < w1) ? wt + kBlock : w1;
-  for (long long wb = wt; wb < wend; wb += whole ? kBlock : kTileW) {
-    // 1. compact the set bits of the (sub-)tile
-    uint32_t bits = 0;
-    const long long w = wb + threadIdx.x;
-    if (whole) bits = tbits;
-    else if (threadIdx.x < kTileW && w < wend) bits = ld_cg_u32(fbc + w);
-    long long total;
-    const long long ex = block_exclusive_scan<kBlock, long long>((long long)__popc(bits), sm.red, &total);
+    long long tsum;
+    const long long tex = block_exclusive_scan<kBlock, long long>((long long)__popc(tbits), sm.red, &tsum);
+  for (long long c0 = 0; c0 < tsum; c0 += kWin) {
+    // 1. list the tile's set bits numbered [c0, c0 + kWin)
     {
-      int o = (int)ex;
-      while (bits) {
-        const int bp = __ffs(bits) - 1;
-        bits &= bits - 1;
-        sm.wu[o++] = (int)(w * 32 + bp);
+      const long long c1 = c0 + kWin;
+      if (tbits && tex < c1 && tex + __popc(tbits) > c0) {
+        uint32_t bits = tbits;
+        long long o = tex;
+        while (bits) {
+          const int bp = __ffs(bits) - 1;
+          bits &= bits - 1;
+          if (o >= c0 && o < c1) sm.wu[o - c0] = (int)(w * 32 + bp);
+          ++o;
+        }
       }
     }
     __syncthreads();
-    const int n = (int)total;
-    if (n == 0) continue;
+    const int n = (int)((tsum - c0 < kWin) ? tsum - c0 : kWin);
     // 2. degrees and CSR offsets; heavy vertices are deferred
     constexpr int PER = (kWin + kBlock - 1) / kBlock;
     const int i0 = threadIdx.x * PER;
@@ -737,7 +750,9 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
       const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
       int found = -1, found2 = -1;
       long long e = e0;
-      if (p.bu_mode == 1) {  // streaming (L1-bypassing) neighbour loads
+      if (p.bu_mode == 2) {  // four at a time, streaming loads
+        probe_range<4, false, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+      } else if (p.bu_mode == 1) {  // streaming (L1-bypassing) neighbour loads
         probe_range<2, false, ASYNC>(p, fbc, fbn, e, e0 + 2 < e1 ? e0 + 2 : e1, found, found2);
         if (found < 0) probe_range<4, false, ASYNC>(p, fbc, fbn, e, e0 + 6 < e1 ? e0 + 6 : e1, found, found2);
         if (found < 0) probe_range<8, false, ASYNC>(p, fbc, fbn, e, e1, found, found2);
@@ -822,20 +837,33 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
   if (threadIdx.x < 3) sm.cnt[threadIdx.x] = 0;
   __syncthreads();
 
-  PolicyState ps;
-  ps.count_prev = 0;
-  ps.is_change = 0;
-  ps.td_adaptive = kInfinite;
-  ps.hub_before = 0;
-  ps.hub_after = 0;
-  ps.tag_prev = 0;
-  ps.bu_dir = 0;
-  ps.n_prev = 1;
-  ps.prev_strategy = XBFS_TD_QUEUE;
-  long long vis_n = 0, vis_m = 0;  // sums over frontiers <= L (thread 0)
-  // statistics of the whole traversal, kept by thread 0 of block 0
-  unsigned long long st_reached = 0, st_msum = 0, st_async = 0;
-  int st_strat[3] = {0, 0, 0};
+  // Policy state and running sums live in shared memory, owned by thread 0:
+  // kept in registers they would be carried by every thread through every
+  // inner loop of the level.
+  LoopState& ls = sm.ls;
+  if (threadIdx.x == 0) {
+    ls.ps.count_prev = 0;
+    ls.ps.is_change = 0;
+    ls.ps.td_adaptive = kInfinite;
+    ls.ps.hub_before = 0;
+    ls.ps.hub_after = 0;
+    ls.ps.tag_prev = 0;
+    ls.ps.bu_dir = 0;
+    ls.ps.n_prev = 1;
+    ls.ps.prev_strategy = XBFS_TD_QUEUE;
+    ls.vis_n = 0;
+    ls.vis_m = 0;
+    ls.st_reached = 0;
+    ls.st_msum = 0;
+    ls.st_async = 0;
+    for (int k = 0; k < 3; ++k) ls.st_strat[k] = 0;
+    if (p.resume) {
+      const ResumeState r = *p.rs;
+      ls.vis_n = r.vis_n;
+      ls.vis_m = r.vis_m;
+      ls.ps = r.ps;
+    }
+  }
 
   bool q_valid = true, b_valid = true;
   unsigned dirty = 1u;  // fb[i] may contain set bits
@@ -849,10 +877,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
     q_valid = r.q_valid != 0;
     b_valid = r.b_valid != 0;
     dirty = r.dirty;
-    vis_n = r.vis_n;
-    vis_m = r.vis_m;
-    ps = r.ps;
   }
+  __syncthreads();
   for (;; ++L) {
     if (L >= p.stop_level) {
       if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -861,9 +887,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         r.q_valid = q_valid;
         r.b_valid = b_valid;
         r.dirty = dirty;
-        r.vis_n = vis_n;
-        r.vis_m = vis_m;
-        r.ps = ps;
+        r.vis_n = ls.vis_n;
+        r.vis_m = ls.vis_m;
+        r.ps = ls.ps;
         *p.rs = r;
       }
       break;
@@ -889,15 +915,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       sm.spec = m_f <= kSpecEdges ? 1 : 0;
       int s = -1;
       if (n_f > 0) {
-        vis_n += n_f;
-        vis_m += m_f;
+        ls.vis_n += n_f;
+        ls.vis_m += m_f;
         if (blockIdx.x == 0) {
-          st_reached += n_f;
-          st_msum += m_f;
-          st_async += own_pend;
+          ls.st_reached += n_f;
+          ls.st_msum += m_f;
+          ls.st_async += own_pend;
         }
-        long long n_u = p.n_ni - vis_n - pn;
-        long long m_u = p.E - vis_m - pm;
+        long long n_u = p.n_ni - ls.vis_n - pn;
+        long long m_u = p.E - ls.vis_m - pm;
         if (n_u < 0) n_u = 0;
         if (m_u < 0) m_u = 0;
         switch (p.policy) {
@@ -908,13 +934,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
             break;
           }
           case XBFS_POLICY_BEAMER:
-            s = decide_beamer(ps, n_f, m_f, m_u, p.V, p.beamer_alpha, p.beamer_beta);
+            s = decide_beamer(ls.ps, n_f, m_f, m_u, p.V, p.beamer_alpha, p.beamer_beta);
             break;
           case XBFS_POLICY_MLP:
             s = -2;  // decided by warp 0 below
             break;
           default:
-            s = decide_reference(ps, L, m_f, p.E, p.alpha);
+            s = decide_reference(ls.ps, L, m_f, p.E, p.alpha);
         }
         if (s == XBFS_BU && !p.allow_bu) s = XBFS_TD_QUEUE;
         if (s == -2) {
@@ -923,8 +949,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
           sm.mlp_h[0][2] = flog((double)n_u);
           sm.mlp_h[0][3] = flog((double)m_u);
           sm.mlp_h[0][4] = flog((double)L);
-          sm.mlp_h[0][5] = (float)ps.prev_strategy;
-          sm.mlp_h[0][6] = (float)(log((double)n_f + 1.0) - log((double)ps.n_prev + 1.0));
+          sm.mlp_h[0][5] = (float)ls.ps.prev_strategy;
+          sm.mlp_h[0][6] = (float)(log((double)n_f + 1.0) - log((double)ls.ps.n_prev + 1.0));
           sm.mlp_h[0][7] = flog((double)m_f / (double)n_f);
         }
         if (blockIdx.x == 0 && L < p.hist_cap) {
@@ -937,7 +963,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
           r.t1 = 0;
           if (L > 0 && L - 1 < p.hist_cap) p.hist[L - 1].t1 = r.t0;
         }
-        ps.n_prev = n_f;
+        ls.ps.n_prev = n_f;
       }
       sm.strategy = s;
     }
@@ -956,10 +982,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
     const int S = sm.strategy;
     if (S < 0) break;  // empty frontier: done
     if (threadIdx.x == 0) {
-      ps.prev_strategy = S;
+      ls.ps.prev_strategy = S;
       if (blockIdx.x == 0) {
         if (L < p.hist_cap) p.hist[L].strategy = S;
-        st_strat[S] += 1;
+        ls.st_strat[S] += 1;
         // counter used at level L+1 (last used at level L-1)
         ctl->heavy[(L + 1) & 1] = 0ull;
       }
@@ -1029,10 +1055,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     ctl->depth = (int)L;
     // a stepped launch adds its levels to what earlier launches counted
-    ctl->reached += st_reached;
-    ctl->msum += st_msum;
-    ctl->n_async += st_async;
-    for (int k = 0; k < 3; ++k) ctl->strat_count[k] += st_strat[k];
+    ctl->reached += ls.st_reached;
+    ctl->msum += ls.st_msum;
+    ctl->n_async += ls.st_async;
+    for (int k = 0; k < 3; ++k) ctl->strat_count[k] += ls.st_strat[k];
     if (L > 0 && L - 1 < p.hist_cap) p.hist[L - 1].t1 = globaltimer_ns();
   }
 }
