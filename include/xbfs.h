@@ -88,8 +88,9 @@ typedef struct xbfs_opts {
                            reference is wrong for padding > 1) */
   float beamer_alpha;   /* XBFS_POLICY_BEAMER: TD->BU when m_f > m_u/alpha (14) */
   float beamer_beta;    /*                     BU->TD when n_f < V/beta (24)   */
-  int32_t bu_probe;     /* bottom-up neighbour loads: 0 = through L1 (default),
-                           1 = streaming (L1 bypass) */
+  int32_t bu_probe;     /* bottom-up neighbour loads: 0 = 2, 4, then 8 at a time
+                           through L1 (default); 1 = the same, streaming (L1
+                           bypass); 2 = 4 at a time, streaming */
   int32_t wait_timeout_us; /* bound of every device-side wait of a traversal
                               (grid barriers); 0 = 10 s. On expiry the call
                               returns XBFS_ERR_DEVICE_TIMEOUT */
