@@ -149,6 +149,15 @@ xbfs_status xbfs_graph_info(const xbfs_graph* g, int64_t* V, int64_t* E, int64_t
 /* Copy the device CSR back to host buffers (beg: V+1, csr: E entries; csr
  * may be NULL to fetch the offsets only). */
 xbfs_status xbfs_graph_download(const xbfs_graph* g, int64_t* beg, int32_t* csr);
+/* Reorders the neighbours inside every vertex's CSR segment (the offsets and
+ * the edge multiset stay the same). XBFS_ADJ_DEGREE_DESC puts high-degree
+ * neighbours first, so bottom-up steps on power-law graphs find a frontier
+ * parent in fewer probes; XBFS_ADJ_ID_ASC restores ascending ids. Levels
+ * never depend on the order (parents may). No reference counterpart: the
+ * reference traverses the file order. Needs about 20 bytes per edge of
+ * temporary device memory; xbfs_graph_download returns the new order. */
+enum { XBFS_ADJ_ID_ASC = 0, XBFS_ADJ_DEGREE_DESC = 1 };
+xbfs_status xbfs_graph_sort_adjacency(xbfs_graph* g, int32_t order);
 /* Write the handle's CSR in the reference's file format. */
 xbfs_status xbfs_graph_save(const xbfs_graph* g, const char* beg_path, const char* csr_path);
 void xbfs_graph_free(xbfs_graph* g);

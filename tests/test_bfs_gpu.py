@@ -202,3 +202,43 @@ def test_many_sources_pipelined_equal_single_calls(out):
         mc += oracle.edges_mc(beg, ref)
     assert r.edges_mc == mc
     g.free()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bu_mode", [0, 1, 2, 3])
+def test_bottom_up_probe_modes(bu_mode):
+    """Every bottom-up probe shape gives the oracle's levels and a valid tree
+    (R-MAT with async bottom-up on and off, and a forced all-bottom-up run)."""
+    beg, csr = gen_rmat_host(16, 16, 23)
+    g = Graph.from_csr(beg, csr)
+    for s in pick_sources(beg, 3, 8):
+        ref = oracle.bfs_queue(beg, csr, int(s))
+        for kw in ({}, {"async_bu": False}, {"policy": "forced", "forced": ["td_queue", "bu"]}):
+            r = g.bfs(int(s), want_parents=True, bu_mode=bu_mode, **kw)
+            assert np.array_equal(r.levels, ref), (bu_mode, kw)
+            assert oracle.check_tree(beg, csr, int(s), r.levels, r.parents) == 0
+    g.free()
+
+
+@pytest.mark.gpu
+def test_degree_sorted_adjacency_keeps_levels():
+    """xbfs_graph_sort_adjacency: segments become degree-descending
+    permutations of themselves, traversal levels stay the oracle's (parents
+    stay a valid tree), and sorting by id restores the generator's CSR."""
+    beg, csr = gen_rmat_host(15, 16, 41)
+    g = Graph.from_csr(beg, csr)
+    g.sort_adjacency("degree")
+    b2, c2 = g.download()
+    assert np.array_equal(b2, beg)
+    deg = np.diff(beg)
+    for u in np.random.default_rng(0).integers(0, len(beg) - 1, size=300):
+        seg, seg2 = csr[beg[u]:beg[u + 1]], c2[beg[u]:beg[u + 1]]
+        assert np.array_equal(np.sort(seg), np.sort(seg2))
+        assert np.all(np.diff(deg[seg2]) <= 0)
+    for s in pick_sources(beg, 4, 3):
+        r = g.bfs(int(s), want_parents=True)
+        assert np.array_equal(r.levels, oracle.bfs_queue(beg, csr, int(s)))
+        assert oracle.check_tree(beg, csr, int(s), r.levels, r.parents) == 0
+    g.sort_adjacency("id")
+    assert np.array_equal(g.download()[1], csr)
+    g.free()

@@ -123,6 +123,7 @@ SIGNATURES = {
     "xbfs_bfs": (_i32, [_p, _i32, _p, _p, C.POINTER(Opts), C.POINTER(Stats)]),
     "xbfs_bfs_noalloc": (_i32, [_p, _i32, _p, _p, C.POINTER(Opts), C.POINTER(Stats)]),
     "xbfs_bfs_many": (_i32, [_p, _p, _i32, _p, C.POINTER(Opts), C.POINTER(Stats)]),
+    "xbfs_graph_sort_adjacency": (_i32, [_p, _i32]),
     "xbfs_last_trace": (_i32, [_p, C.POINTER(LevelTrace), _i32, _PI32]),
     "xbfs_gen_rmat": (_i32, [_i32, _i32, _u64, _f64, _f64, _f64, _i32, C.POINTER(_p)]),
     "xbfs_gen_grid": (_i32, [_i32, _i32, _i32, C.POINTER(_p)]),

@@ -212,6 +212,11 @@ class Graph:
                          strategies={"td_queue": st.n_td_queue, "td_scan": st.n_td_scan, "bu": st.n_bu},
                          n_async=st.n_async, trace=trace)
 
+    def sort_adjacency(self, order: str = "degree") -> None:
+        """Reorder neighbours within each CSR segment: "degree" (descending
+        neighbour degree, fewer bottom-up probes) or "id" (ascending ids)."""
+        check(lib.xbfs_graph_sort_adjacency(self._h, {"id": 0, "degree": 1}[order]))
+
     def bfs_many(self, srcs, levels=None, opts: Optional[BfsOptions] = None, **kw) -> BfsResult:
         """One single-source traversal per source, pipelined with the copies of
         their level arrays (xbfs_bfs_many): levels[i] belongs to srcs[i] (n x V

@@ -705,6 +705,74 @@ __device__ __forceinline__ void probe_range(const Params& p, const uint32_t* fbc
   }
 }
 
+// Two vertices per lane: the same probe for vertex pairs, with the loads of
+// both issued together, so a lane has two dependency chains in flight.
+template <int PW, bool ASYNC>
+__device__ __forceinline__ void probe_pair(const Params& p, const uint32_t* fbc, const uint32_t* fbn,
+                                           long long (&e)[2], const long long (&lim)[2], int (&found)[2],
+                                           int (&found2)[2]) {
+  for (;;) {
+    bool act[2];
+    act[0] = found[0] < 0 && e[0] < lim[0];
+    act[1] = found[1] < 0 && e[1] < lim[1];
+    if (!act[0] && !act[1]) return;
+    int u[2][PW];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int k = 0; k < PW; ++k) u[j][k] = (act[j] && e[j] + k < lim[j]) ? __ldg(p.csr + e[j] + k) : -1;
+    uint32_t wc[2][PW];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int k = 0; k < PW; ++k) wc[j][k] = (u[j][k] >= 0) ? fbc[u[j][k] >> 5] : 0u;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int k = 0; k < PW; ++k)
+        if (found[j] < 0 && u[j][k] >= 0 && ((wc[j][k] >> (u[j][k] & 31)) & 1u)) found[j] = u[j][k];
+    if (ASYNC) {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        if (!act[j] || found[j] >= 0 || found2[j] >= 0) continue;
+#pragma unroll
+        for (int k = 0; k < PW; ++k)
+          if (found2[j] < 0 && u[j][k] >= 0 && ((ld_cg_u32(fbn + (u[j][k] >> 5)) >> (u[j][k] & 31)) & 1u))
+            found2[j] = u[j][k];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      if (act[j]) e[j] += PW;
+  }
+}
+
+// Publishes a warp's bottom-up results for 32 consecutive entries of a sorted
+// list: vertices sharing a bitmap word sit in adjacent lanes, so their bits
+// are ORed along each run of equal words and the run's first lane issues one
+// atomic per word instead of one per vertex.
+template <bool ASYNC>
+__device__ __forceinline__ void bu_publish_words(const Params& p, uint32_t* fbn, uint32_t* fbn2, uint32_t word,
+                                                 uint32_t m1, uint32_t m2, bool valid) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t ow = __shfl_down_sync(0xffffffffu, word, off);
+    const uint32_t o1 = __shfl_down_sync(0xffffffffu, m1, off);
+    const uint32_t o2 = __shfl_down_sync(0xffffffffu, m2, off);
+    if (lane + off < 32 && ow == word) {
+      m1 |= o1;
+      m2 |= o2;
+    }
+  }
+  const uint32_t pw = __shfl_up_sync(0xffffffffu, word, 1);
+  if (valid && (lane == 0 || pw != word)) {
+    if (m1 | m2) red_or_u32(p.vis + word, m1 | m2);
+    if (m1) red_or_u32(fbn + word, m1);
+    if (ASYNC && m2) red_or_u32(fbn2 + word, m2);
+  }
+}
+
 // Bottom-up step for level L. Each CTA owns a contiguous slice of the vertex
 // range (vertex ids are scrambled, so slices carry similar work): it compacts
 // the slice's unvisited vertices into a sorted list with block ballot /
@@ -738,6 +806,62 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
   __syncthreads();
   const int n = (int)pos;
   const int lane = threadIdx.x & 31;
+  if (p.bu_mode == 3) {
+    // 64 list entries per warp grab, two per lane (entries base+lane and
+    // base+32+lane), probed together: 2, then 4 neighbours at a time
+    for (;;) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&sm.bu_next, 64);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= n) break;
+      int v[2];
+      long long eb[2], ee[2], e[2], lim[2];
+      int found[2] = {-1, -1}, found2[2] = {-1, -1};
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int i = base + 32 * j + lane;
+        v[j] = (i < n) ? list[i] : -1;
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        eb[j] = 0;
+        ee[j] = 0;
+        if (v[j] >= 0) {
+          eb[j] = ld_nc_i64(p.beg + v[j]);
+          ee[j] = ld_nc_i64(p.beg + v[j] + 1);
+        }
+        e[j] = eb[j];
+        lim[j] = eb[j] + 2 < ee[j] ? eb[j] + 2 : ee[j];
+      }
+      probe_pair<2, ASYNC>(p, fbc, fbn, e, lim, found, found2);
+      lim[0] = ee[0];
+      lim[1] = ee[1];
+      probe_pair<4, ASYNC>(p, fbc, fbn, e, lim, found, found2);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        uint32_t word = 0xffffffffu, m1 = 0, m2 = 0;
+        if (v[j] >= 0) {
+          word = (uint32_t)v[j] >> 5;
+          const uint32_t bit = 1u << (v[j] & 31);
+          if (found[j] >= 0) {
+            p.levels[v[j]] = L + 1;
+            if (PAR) p.parents[v[j]] = found[j];
+            m1 = bit;
+            acc.n1 += 1;
+            acc.m1 += ee[j] - eb[j];
+          } else if (ASYNC && found2[j] >= 0) {
+            p.levels[v[j]] = L + 2;
+            if (PAR) p.parents[v[j]] = found2[j];
+            m2 = bit;
+            acc.n2 += 1;
+            acc.m2 += ee[j] - eb[j];
+          }
+        }
+        bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, m2, v[j] >= 0);
+      }
+    }
+    return;
+  }
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&sm.bu_next, 32);

@@ -82,6 +82,7 @@ struct Graph {
   int64_t max_degree = 0;
   int64_t n_isolated = 0;
   bool symmetric = true;         // edge multiset symmetric: bottom-up steps allowed
+  int adj_order = -1;            // XBFS_ADJ_* after xbfs_graph_sort_adjacency, -1 = as loaded
   int64_t cnt_deg_gt[16] = {0};  // vertices with degree > 2^k, k = 0..15
   DevBuf beg;                    // int64[V+1]
   DevBuf csr;                    // int32[E] (+16 bytes tail padding)
