@@ -200,8 +200,9 @@ struct __align__(16) Smem {
   unsigned long long base_slot, base_edge;
   long long red[kBlock / 32 + 1];
   long long red4[4 * (kBlock / 32)];
-  float mlp_h[2][32];
+  float mlp_raw[8];             // statistics the learned switch's features come from
   LoopState ls;
+  float mlp_w[1464];            // the learned switch's weights (XBFS_POLICY_MLP); must stay last
 };
 
 // Loop state carried across launches in stepped mode (xbfs_level_costs): a
@@ -269,44 +270,65 @@ __device__ int decide_beamer(PolicyState& ps, long long n_f, long long m_f, long
   return ps.bu_dir ? XBFS_BU : XBFS_TD_QUEUE;
 }
 
-// MLP inference (8 -> 32 -> 32 -> 3), one warp, weights packed as
-// [mean 8][std 8][W1 32x8][b1 32][W2 32x32][b2 32][W3 3x32][b3 3].
-__device__ int mlp_decide(const float* w, const float feat[8], float* h1s, float* h2s, int lane) {
-  const float* mean = w;
-  const float* sd = w + 8;
-  const float* W1 = w + 16;
-  const float* B1 = W1 + 256;
-  const float* W2 = B1 + 32;
-  const float* B2 = W2 + 1024;
+// MLP inference (8 -> 32 -> 32 -> 3), one warp, from a shared-memory copy of
+// the weights made once per launch (mlp_stage). The packed global layout is
+// [mean 8][std 8][W1 32x8][b1 32][W2 32x32][b2 32][W3 3x32][b3 3]; in shared
+// memory W1 and W2 are stored transposed (input-major), so that lane j
+// reading row j of either walks consecutive banks instead of one bank.
+constexpr int kMlpParams = 16 + 256 + 32 + 1024 + 32 + 96 + 3;  // 1459
+
+__device__ void mlp_stage(const float* __restrict__ w, float* sw) {
+  for (int t = threadIdx.x; t < kMlpParams; t += blockDim.x) {
+    int d = t;
+    if (t >= 16 && t < 16 + 256) {  // W1[j][i] -> W1T[i][j]
+      const int j = (t - 16) / 8, i = (t - 16) % 8;
+      d = 16 + i * 32 + j;
+    } else if (t >= 304 && t < 304 + 1024) {  // W2[j][i] -> W2T[i][j]
+      const int j = (t - 304) / 32, i = (t - 304) % 32;
+      d = 304 + i * 32 + j;
+    }
+    sw[d] = w[t];
+  }
+}
+
+// Features (log1p of n_f, m_f, n_u, m_u and the level; the previous
+// strategy; log growth of the frontier; log1p of its mean degree), one per
+// lane, then the three layers with the hidden activations passed by shuffles.
+// Called by one full warp.
+__device__ int mlp_decide(const float* sw, const float* raw, int lane) {
+  const float* mean = sw;
+  const float* sd = sw + 8;
+  const float* W1T = sw + 16;
+  const float* B1 = W1T + 256;
+  const float* W2T = B1 + 32;
+  const float* B2 = W2T + 1024;
   const float* W3 = B2 + 32;
   const float* B3 = W3 + 96;
-  float x[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) x[i] = (feat[i] - mean[i]) / sd[i];
+  float f = 0.f;
+  if (lane < 8) {
+    const float r = raw[lane];
+    if (lane == 5) f = r;
+    else if (lane == 6) f = logf(raw[0] + 1.f) - logf(raw[6] + 1.f);
+    else f = log1pf(r > 0.f ? r : 0.f);
+    f = (f - mean[lane]) / sd[lane];
+  }
   float a = B1[lane];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) a = fmaf(W1[lane * 8 + i], x[i], a);
+  for (int i = 0; i < 8; ++i) a = fmaf(W1T[i * 32 + lane], __shfl_sync(0xffffffffu, f, i), a);
   a = fmaxf(a, 0.f);
-  h1s[lane] = a;
-  __syncwarp();
   float b = B2[lane];
-  for (int i = 0; i < 32; ++i) b = fmaf(W2[lane * 32 + i], h1s[i], b);
+#pragma unroll 8
+  for (int i = 0; i < 32; ++i) b = fmaf(W2T[i * 32 + lane], __shfl_sync(0xffffffffu, a, i), b);
   b = fmaxf(b, 0.f);
-  h2s[lane] = b;
-  __syncwarp();
   float o[3];
-  for (int k = 0; k < 3; ++k) {
-    float t = W3[k * 32 + lane] * b;
-    t = warp_sum(t);
-    o[k] = t + B3[k];
-  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) o[k] = warp_sum(W3[k * 32 + lane] * b) + B3[k];
   int best = 0;
   if (o[1] > o[best]) best = 1;
   if (o[2] > o[best]) best = 2;
   return best;
 }
 
-__device__ __forceinline__ float flog(double x) { return (float)log1p(x > 0 ? x : 0.0); }
 
 // ---------------------------------------------------------------------------
 // Staging of top-down winners (per CTA) and flush to the global binned queue.
@@ -959,6 +981,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
   Ctl* ctl = p.ctl;
   if (p.absent_block > 0 && (int)blockIdx.x == p.absent_block - 1) return;  // test hook: never arrives
   if (threadIdx.x < 3) sm.cnt[threadIdx.x] = 0;
+  if (p.policy == XBFS_POLICY_MLP && p.mlp) mlp_stage(p.mlp, sm.mlp_w);
   __syncthreads();
 
   // Policy state and running sums live in shared memory, owned by thread 0:
@@ -1068,14 +1091,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         }
         if (s == XBFS_BU && !p.allow_bu) s = XBFS_TD_QUEUE;
         if (s == -2) {
-          sm.mlp_h[0][0] = flog((double)n_f);
-          sm.mlp_h[0][1] = flog((double)m_f);
-          sm.mlp_h[0][2] = flog((double)n_u);
-          sm.mlp_h[0][3] = flog((double)m_u);
-          sm.mlp_h[0][4] = flog((double)L);
-          sm.mlp_h[0][5] = (float)ls.ps.prev_strategy;
-          sm.mlp_h[0][6] = (float)(log((double)n_f + 1.0) - log((double)ls.ps.n_prev + 1.0));
-          sm.mlp_h[0][7] = flog((double)m_f / (double)n_f);
+          // raw statistics; every warp forms the features and runs the network
+          sm.mlp_raw[0] = (float)n_f;
+          sm.mlp_raw[1] = (float)m_f;
+          sm.mlp_raw[2] = (float)n_u;
+          sm.mlp_raw[3] = (float)m_u;
+          sm.mlp_raw[4] = (float)L;
+          sm.mlp_raw[5] = (float)ls.ps.prev_strategy;
+          sm.mlp_raw[6] = (float)ls.ps.n_prev;
+          sm.mlp_raw[7] = (float)((double)m_f / (double)n_f);
         }
         if (blockIdx.x == 0 && L < p.hist_cap) {
           LevelRecDev& r = p.hist[L];
@@ -1093,13 +1117,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
     }
     __syncthreads();
     if (sm.strategy == -2) {
+      // the learned switch: warp 0 evaluates it while the block waits (one
+      // warp keeps the shared-memory and shuffle traffic of the network small)
       if (threadIdx.x < 32) {
-        float feat[8];
-        for (int i = 0; i < 8; ++i) feat[i] = sm.mlp_h[0][i];
-        __syncwarp();
-        int s = p.mlp ? mlp_decide(p.mlp, feat, sm.mlp_h[0], sm.mlp_h[1], threadIdx.x) : XBFS_TD_QUEUE;
-        if (s == XBFS_BU && !p.allow_bu) s = XBFS_TD_QUEUE;
-        if (threadIdx.x == 0) sm.strategy = s;
+        int s2 = p.mlp ? mlp_decide(sm.mlp_w, sm.mlp_raw, threadIdx.x) : XBFS_TD_QUEUE;
+        if (s2 == XBFS_BU && !p.allow_bu) s2 = XBFS_TD_QUEUE;
+        if (threadIdx.x == 0) sm.strategy = s2;
       }
       __syncthreads();
     }
@@ -1309,8 +1332,10 @@ static xbfs_status setup_params(Graph* g, const xbfs_opts& o, int* d_levels, int
 
   const bool par_on = d_parents != nullptr;
   const void* kfn = par_on ? (const void*)k_bfs<true> : (const void*)k_bfs<false>;
-  const size_t smem = sizeof(Smem);
-  XBFS_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the weight copy of the learned switch sits at the end of Smem and is only
+  // allocated for launches that use it (shared memory taken from L1)
+  const size_t smem = sizeof(Smem) - (p.policy == XBFS_POLICY_MLP ? 0 : sizeof(((Smem*)0)->mlp_w));
+  XBFS_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)));
   int nsm = 0, per_sm = 0;
   XBFS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device));
   XBFS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kBlock, smem));
