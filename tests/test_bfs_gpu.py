@@ -183,15 +183,34 @@ def test_load_file_pair_and_malformed_inputs(tmp_path):
     assert e.value.status == _lib.XBFS_ERR_FORMAT
 
 
+def _path_graph(n):
+    beg = np.zeros(n + 1, dtype=np.int64)
+    deg = np.full(n, 2, dtype=np.int64)
+    deg[0] = deg[-1] = 1
+    beg[1:] = np.cumsum(deg)
+    csr = np.empty(beg[-1], dtype=np.int32)
+    for u in range(n):
+        nb = [v for v in (u - 1, u + 1) if 0 <= v < n]
+        csr[beg[u]:beg[u + 1]] = nb
+    return beg, csr
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("out", ["host", "device"])
-def test_many_sources_pipelined_equal_single_calls(out):
+@pytest.mark.parametrize("out,kind", [("host", "rmat"), ("device", "rmat"), ("host", "grid"), ("host", "path")])
+def test_many_sources_pipelined_equal_single_calls(out, kind):
     """xbfs_bfs_many: n traversals with the level copies overlapped; every row
-    equals the oracle and the single-call result for its source."""
+    equals the oracle for its source. Host rows travel as 8-bit levels (R-MAT,
+    < 256 levels), 16-bit (a grid with ~500 levels) or full width (a path of
+    70,000 levels)."""
     import torch
-    beg, csr = gen_rmat_host(15, 16, 31)
+    if kind == "rmat":
+        beg, csr = gen_rmat_host(15, 16, 31)
+    elif kind == "grid":
+        beg, csr = gen_grid_host(300, 200)
+    else:
+        beg, csr = _path_graph(70000)
     g = Graph.from_csr(beg, csr)
-    srcs = pick_sources(beg, 7, 5)
+    srcs = pick_sources(beg, 7, 5) if kind != "path" else np.array([0, 69999], dtype=np.int32)
     lv = None if out == "host" else torch.empty((len(srcs), g.V), dtype=torch.int32, device="cuda:0")
     r = g.bfs_many(srcs, levels=lv)
     rows = r.levels if out == "host" else r.levels.cpu().numpy()
