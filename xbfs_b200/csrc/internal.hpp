@@ -34,6 +34,8 @@ struct DevBuf {
 struct PinnedBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(p); }
   ~PinnedBuf() {
     if (p) cudaFreeHost(p);
   }

@@ -284,8 +284,11 @@ struct SlotBatch {
   unsigned long long busy = 0;
   std::deque<int> waiting;
   int k_ticks = 1;
-  std::vector<int> depths;
   int grid = 0;
+  bool inflight = false;         // a round of ticks is on the stream
+  int round_k = 0;               // its length
+  long long issued = 0;          // first tick not yet issued
+  cudaEvent_t ev = nullptr;      // end of the round in flight
 };
 
 struct Server {
@@ -296,11 +299,13 @@ struct Server {
   std::vector<ServeRequest> reqs;
   ~Server() {
     DeviceGuard dg(device);
-    for (auto& b : batches)
+    for (auto& b : batches) {
       if (b->stream) {
         cudaStreamSynchronize(b->stream);
         cudaStreamDestroy(b->stream);
       }
+      if (b->ev) cudaEventDestroy(b->ev);
+    }
   }
 };
 
@@ -346,13 +351,16 @@ static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
   return XBFS_OK;
 }
 
-static xbfs_status batch_ticks(SlotBatch& b, int k) {
+// Issues k ticks on the batch's stream with `grid` blocks per tick kernel
+// (sized by the caller from the frontier; the kernels are grid-stride, so a
+// frontier that outgrows it is still covered).
+static xbfs_status batch_ticks(SlotBatch& b, int k, int grid) {
   for (int i = 0; i < k; ++i) {
     const long long t = b.tick + i;
     sv::k_sv_reset<<<1, 32, 0, b.stream>>>(b.p, t);
-    sv::k_sv_expand<<<b.grid, sv::kBlock, 0, b.stream>>>(b.p, t);
-    sv::k_sv_merge<<<b.grid, sv::kBlock, 0, b.stream>>>(b.p, t);
-    sv::k_sv_retire<<<b.grid, 256, 0, b.stream>>>(b.p, t);
+    sv::k_sv_expand<<<grid, sv::kBlock, 0, b.stream>>>(b.p, t);
+    sv::k_sv_merge<<<grid, sv::kBlock, 0, b.stream>>>(b.p, t);
+    sv::k_sv_retire<<<grid, 256, 0, b.stream>>>(b.p, t);
   }
   XBFS_CUDA_TRY(cudaGetLastError());
   return XBFS_OK;
@@ -437,7 +445,17 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
   const auto t0 = std::chrono::steady_clock::now();
   size_t next = 0;
   int done = 0;
-  std::vector<sv::Ctl> hctl(nb);
+  // every batch advances in rounds of up to kRing ticks; a round is issued,
+  // its end marked by an event, and processed when that event has passed, so
+  // a batch with short traversals is never held up by one with long ones
+  PinnedBuf hctl_buf;
+  if (xbfs_status st = hctl_buf.ensure(sizeof(sv::Ctl) * (size_t)nb)) return st;
+  sv::Ctl* hctl = hctl_buf.as<sv::Ctl>();
+  for (auto& bp : srv->batches) {
+    bp->inflight = false;
+    bp->issued = bp->tick;
+    if (!bp->ev) XBFS_CUDA_TRY(cudaEventCreateWithFlags(&bp->ev, cudaEventDisableTiming));
+  }
   const double last_arrival = n ? srv->reqs[order.back()].arrival_us : 0.0;
   while (done < n) {
     const double now = now_us(t0);
@@ -448,7 +466,62 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
       srv->batches[srv->reqs[order[next]].graph]->waiting.push_back(order[next]);
       ++next;
     }
-    // admission: a free slot and room in the HBM budget
+    // completed rounds: find the slots that gained nothing at some tick
+    for (int gi = 0; gi < nb; ++gi) {
+      SlotBatch& b = *srv->batches[gi];
+      if (!b.inflight) continue;
+      const cudaError_t q = cudaEventQuery(b.ev);
+      if (q == cudaErrorNotReady) continue;
+      XBFS_CUDA_TRY(q);
+      b.inflight = false;
+      const int k = b.round_k;
+      unsigned long long finished = 0;
+      for (int i = 0; i < k; ++i) {
+        const long long t = b.tick + i;
+        const unsigned long long act = hctl[gi].active[t % sv::kRing];
+        // slots joined at or before t that gained nothing at t are complete
+        for (unsigned long long m = b.busy & ~finished; m; m &= m - 1) {
+          const int sl = __builtin_ctzll(m);
+          const ServeRequest& r = srv->reqs[b.req_of_slot[sl]];
+          if (r.join <= t && !((act >> sl) & 1ull)) finished |= 1ull << sl;
+        }
+      }
+      b.tick += k;
+      if (!finished) {
+        b.k_ticks = std::min(sv::kRing, b.k_ticks * 2);
+        continue;
+      }
+      const double tf = now_us(t0);
+      int max_depth = 0;
+      for (unsigned long long m = finished; m; m &= m - 1) {
+        const int sl = __builtin_ctzll(m);
+        ServeRequest& r = srv->reqs[b.req_of_slot[sl]];
+        r.finish_us = tf;
+        r.status = 2;
+        r.msum = hctl[gi].msum[sl];
+        max_depth = std::max<int>(max_depth, (int)(b.tick - r.join));
+        if (keep_outputs == 2)  // deliver to the caller's host array, then give the memory back
+          XBFS_CUDA_TRY(cudaMemcpyAsync(levels[b.req_of_slot[sl]], r.out, (size_t)b.g->V * 4, cudaMemcpyDeviceToHost,
+                                        b.stream));
+        if (keep_outputs != 1) {
+          XBFS_CUDA_TRY(cudaFreeAsync(r.out, b.stream));
+          srv->in_use -= (size_t)b.g->V * 4;
+          r.out = nullptr;
+        }
+        int* null = nullptr;
+        XBFS_CUDA_TRY(cudaMemcpyAsync(b.out_tab.as<int*>() + sl, &null, sizeof(int*), cudaMemcpyHostToDevice, b.stream));
+        b.req_of_slot[sl] = -1;
+        ++done;
+      }
+      sv::k_sv_clear<<<b.grid, 256, 0, b.stream>>>(b.p, finished);
+      XBFS_CUDA_TRY(cudaGetLastError());
+      b.busy &= ~finished;
+      // host every ~1/8 of the depth seen so far, at least every tick
+      b.k_ticks = std::max(1, std::min(sv::kRing, max_depth / 8));
+    }
+    // admission: a free slot and room in the HBM budget; a request joins at
+    // the batch's next unissued tick (its seed is stream-ordered after the
+    // round in flight)
     for (int gi = 0; gi < nb; ++gi) {
       SlotBatch& b = *srv->batches[gi];
       while (!b.waiting.empty() && b.busy != ~0ull) {
@@ -457,35 +530,52 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
         const int ri = b.waiting.front();
         b.waiting.pop_front();
         ServeRequest& r = srv->reqs[ri];
-        const int s = __builtin_ctzll(~b.busy);
-        b.busy |= 1ull << s;
-        b.req_of_slot[s] = ri;
+        const int sl = __builtin_ctzll(~b.busy);
+        b.busy |= 1ull << sl;
+        b.req_of_slot[sl] = ri;
         void* mem = nullptr;
         XBFS_CUDA_TRY(cudaMallocFromPoolAsync(&mem, need, srv->pool, b.stream));
         srv->in_use += need;
         r.out = (int*)mem;
-        r.slot = s;
-        r.join = b.tick;
+        r.slot = sl;
+        r.join = b.issued;
         r.admit_us = now_us(t0);
         r.status = 1;
         XBFS_CUDA_TRY(cudaMemsetAsync(r.out, 0xff, need, b.stream));
-        XBFS_CUDA_TRY(cudaMemcpyAsync(b.out_tab.as<int*>() + s, &r.out, sizeof(int*), cudaMemcpyHostToDevice, b.stream));
-        XBFS_CUDA_TRY(cudaMemcpyAsync(b.join_tab.as<long long>() + s, &r.join, 8, cudaMemcpyHostToDevice, b.stream));
-        // the seed goes into tick b.tick's frontier
-        sv::k_sv_seed<<<1, 32, 0, b.stream>>>(b.p, b.tick, s, r.src);
+        XBFS_CUDA_TRY(cudaMemcpyAsync(b.out_tab.as<int*>() + sl, &r.out, sizeof(int*), cudaMemcpyHostToDevice, b.stream));
+        XBFS_CUDA_TRY(cudaMemcpyAsync(b.join_tab.as<long long>() + sl, &r.join, 8, cudaMemcpyHostToDevice, b.stream));
+        // the seed goes into tick b.issued's frontier
+        sv::k_sv_seed<<<1, 32, 0, b.stream>>>(b.p, b.issued, sl, r.src);
       }
     }
-    // advance every batch with running slots by K ticks (overlapping streams)
+    // issue the next round of every idle batch with running slots
     int running = 0;
     for (int gi = 0; gi < nb; ++gi) {
       SlotBatch& b = *srv->batches[gi];
+      if (b.inflight) {
+        ++running;
+        continue;
+      }
       if (!b.busy) continue;
       ++running;
       const int k = std::max(1, std::min(b.k_ticks, sv::kRing - (int)(b.tick % sv::kRing)));
-      xbfs_status st = batch_ticks(b, k);
+      // Blocks per tick kernel from the frontier the round starts with (4x
+      // headroom for growth inside the round): small frontiers (grids) use a
+      // few SMs, so the batches' streams share the GPU instead of taking turns.
+      int grid = b.grid;
+      if (b.tick > 0) {
+        const unsigned long long pk = hctl[gi].q[b.tick % 3];
+        const unsigned long long work = std::max<unsigned long long>(pk >> 31, pk & sv::kCountMask);
+        const unsigned long long want = (work * 4 + sv::kBlock * 2 - 1) / (sv::kBlock * 2);
+        grid = (int)std::min<unsigned long long>((unsigned long long)b.grid, std::max<unsigned long long>(8, want));
+      }
+      xbfs_status st = batch_ticks(b, k, grid);
       if (st) return st;
       XBFS_CUDA_TRY(cudaMemcpyAsync(&hctl[gi], b.ctl.p, sizeof(sv::Ctl), cudaMemcpyDeviceToHost, b.stream));
-      b.depths.push_back(k);  // ticks issued this round
+      XBFS_CUDA_TRY(cudaEventRecord(b.ev, b.stream));
+      b.round_k = k;
+      b.issued = b.tick + k;
+      b.inflight = true;
     }
     if (!running) {
       // nothing runs, so nothing will give memory back: a request that has
@@ -505,57 +595,6 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
           }
         }
       }
-      continue;
-    }
-    for (int gi = 0; gi < nb; ++gi) {
-      SlotBatch& b = *srv->batches[gi];
-      if (!b.busy) continue;
-      XBFS_CUDA_TRY(cudaStreamSynchronize(b.stream));
-      const int k = b.depths.back();
-      b.depths.pop_back();
-      unsigned long long finished = 0;
-      for (int i = 0; i < k; ++i) {
-        const long long t = b.tick + i;
-        const unsigned long long act = hctl[gi].active[t % sv::kRing];
-        // slots joined at or before t that gained nothing at t are complete
-        for (unsigned long long m = b.busy & ~finished; m; m &= m - 1) {
-          const int s = __builtin_ctzll(m);
-          const ServeRequest& r = srv->reqs[b.req_of_slot[s]];
-          if (r.join <= t && !((act >> s) & 1ull)) finished |= 1ull << s;
-        }
-      }
-      b.tick += k;
-      if (!finished) {
-        b.k_ticks = std::min(sv::kRing, b.k_ticks * 2);
-        continue;
-      }
-      const double tf = now_us(t0);
-      int max_depth = 0;
-      for (unsigned long long m = finished; m; m &= m - 1) {
-        const int s = __builtin_ctzll(m);
-        ServeRequest& r = srv->reqs[b.req_of_slot[s]];
-        r.finish_us = tf;
-        r.status = 2;
-        r.msum = hctl[gi].msum[s];
-        max_depth = std::max<int>(max_depth, (int)(b.tick - r.join));
-        if (keep_outputs == 2)  // deliver to the caller's host array, then give the memory back
-          XBFS_CUDA_TRY(cudaMemcpyAsync(levels[b.req_of_slot[s]], r.out, (size_t)b.g->V * 4, cudaMemcpyDeviceToHost,
-                                        b.stream));
-        if (keep_outputs != 1) {
-          XBFS_CUDA_TRY(cudaFreeAsync(r.out, b.stream));
-          srv->in_use -= (size_t)b.g->V * 4;
-          r.out = nullptr;
-        }
-        int* null = nullptr;
-        XBFS_CUDA_TRY(cudaMemcpyAsync(b.out_tab.as<int*>() + s, &null, sizeof(int*), cudaMemcpyHostToDevice, b.stream));
-        b.req_of_slot[s] = -1;
-        ++done;
-      }
-      sv::k_sv_clear<<<b.grid, 256, 0, b.stream>>>(b.p, finished);
-      XBFS_CUDA_TRY(cudaGetLastError());
-      b.busy &= ~finished;
-      // host every ~1/8 of the depth seen so far, at least every tick
-      b.k_ticks = std::max(1, std::min(sv::kRing, max_depth / 8));
     }
   }
   for (auto& b : srv->batches) XBFS_CUDA_TRY(cudaStreamSynchronize(b->stream));
