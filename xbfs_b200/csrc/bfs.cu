@@ -592,6 +592,106 @@ __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& ac
   }
 }
 
+// Tiny share of the small bin (at most 32 entries for this CTA, the usual case
+// on long-diameter graphs): warp 0 expands it alone with warp scans and
+// shuffles, so the level costs this CTA no block barrier beyond the grid
+// barrier's. Winners go to the next queue with one packed atomic per bin per
+// warp (edges << 31 | count) and the warp's frontier counts straight to f1.
+// Called by warp 0 only; returns nothing to stage or publish afterwards.
+template <bool PAR>
+__device__ void gather_entries_warp(const Params& p, const QOut& q, const QBin& in, unsigned cnt,
+                                    unsigned long long M, unsigned i0, unsigned i1, int L, bool enq, uint32_t* fbn,
+                                    bool spec, FDesc* f1) {
+  const int lane = threadIdx.x & 31;
+  const unsigned i = i0 + lane;
+  const bool own = i < i1;
+  long long d = 0, bg = 0;
+  int u = 0;
+  if (own) {
+    const unsigned long long e0 = in.eb[i];
+    const unsigned long long e1 = (i + 1 < cnt) ? (unsigned long long)in.eb[i + 1] : M;
+    d = (long long)(e1 - e0);
+    u = in.ids[i];
+    bg = in.bg[i];
+  }
+  const long long incl = warp_inclusive_scan(d);
+  const long long ex = incl - d;
+  const long long T = __shfl_sync(0xffffffffu, incl, 31);
+  const int n = (int)(i1 - i0);
+  long long n1 = 0, m1 = 0;
+  for (long long base = 0; base < T; base += 32) {
+    const long long e = base + lane;
+    // owner: the last of the n entries whose exclusive offset is <= e
+    // (branch-free binary search, every lane takes part in every shuffle)
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const int cand = lo + step;
+      const long long exc = __shfl_sync(0xffffffffu, ex, cand < 32 ? cand : 31);
+      if (cand < n && exc <= e) lo = cand;
+    }
+    const long long ex_a = __shfl_sync(0xffffffffu, ex, lo);
+    const long long bg_a = __shfl_sync(0xffffffffu, bg, lo);
+    const int par_u = __shfl_sync(0xffffffffu, u, lo);
+    int v = -1;
+    if (e < T) v = ld_stream_i32(p.csr + bg_a + (e - ex_a));
+    // claim (same rules as claim_td)
+    bool win = false;
+    long long b0 = 0, b1 = 0;
+    uint32_t word = 0, bit = 0;
+    if (v >= 0) {
+      word = (uint32_t)v >> 5;
+      bit = 1u << (v & 31);
+      bool skip = false;
+      if (spec) {
+        b0 = ld_nc_i64(p.beg + v);
+        b1 = ld_nc_i64(p.beg + v + 1);
+      } else {
+        skip = (ld_cg_u32(p.vis + word) & bit) != 0;
+      }
+      if (!skip) win = (atomicOr(p.vis + word, bit) & bit) == 0;
+      if (win) {
+        p.levels[v] = L + 1;
+        if (PAR) p.parents[v] = par_u;
+        if (!spec) {
+          b0 = ld_nc_i64(p.beg + v);
+          b1 = ld_nc_i64(p.beg + v + 1);
+        }
+        n1 += 1;
+        m1 += b1 - b0;
+        if (!enq) red_or_u32(fbn + word, bit);
+      }
+    }
+    if (enq) {
+      const long long dv = b1 - b0;
+      const int bin = win ? bin_of(dv, p.small_max, p.medium_max) : -1;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const bool mine = win && dv > 0 && bin == b;
+        const unsigned mask = __ballot_sync(0xffffffffu, mine);
+        if (!mask) continue;
+        const long long dd = mine ? dv : 0;
+        const long long inc = warp_inclusive_scan(dd);
+        unsigned long long old = 0;
+        if (lane == 31) old = atomicAdd(&q.ctr[b], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
+        old = __shfl_sync(0xffffffffu, old, 31);
+        if (mine) {
+          const unsigned long long slot = (old & kCountMask) + __popc(mask & ((1u << lane) - 1));
+          q.b[b].ids[slot] = v;
+          q.b[b].eb[slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - dd));
+          q.b[b].bg[slot] = b0;
+        }
+      }
+    }
+  }
+  n1 = warp_sum(n1);
+  m1 = warp_sum(m1);
+  if (lane == 0) {
+    if (n1) atomicAdd(&f1->n, (unsigned long long)n1);
+    if (m1) atomicAdd(&f1->m, (unsigned long long)m1);
+  }
+}
+
 // Top-down from a frontier held only as a bitmap ("single scan"): every CTA
 // compacts the set bits of its slice tile by tile into shared memory, gives
 // each vertex of degree <= kHeavyDeg its exclusive edge offset with a block
@@ -1154,18 +1254,29 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       QOut qo;
       for (int b2 = 0; b2 < 3; ++b2) qo.b[b2] = p.q[par ^ 1][b2];
       qo.ctr = F1->bin;
-      if (q_valid) {
-        for (int bin = 2; bin >= 1; --bin) {
-          const unsigned long long pk = sm.bins[bin];
-          gather_bin<PAR>(p, sm, qo, acc, p.q[par][bin], (unsigned)(pk & kCountMask), pk >> 31, (int)L, enq, fbn);
-        }
-        const unsigned long long pk0 = sm.bins[0];
-        gather_entries<PAR>(p, sm, qo, acc, p.q[par][0], (unsigned)(pk0 & kCountMask), pk0 >> 31, (int)L, enq, fbn);
+      // a CTA whose whole share is at most 32 small-bin entries takes the
+      // warp-only path (no staging, no block reductions)
+      const unsigned long long pk0 = sm.bins[0];
+      const unsigned cnt0 = (unsigned)(pk0 & kCountMask);
+      const unsigned i0 = (unsigned)((unsigned long long)cnt0 * blockIdx.x / nb);
+      const unsigned i1 = (unsigned)((unsigned long long)cnt0 * (blockIdx.x + 1) / nb);
+      const bool tiny = q_valid && (sm.bins[1] & kCountMask) == 0 && (sm.bins[2] & kCountMask) == 0 && i1 - i0 <= 32;
+      if (tiny) {
+        if (threadIdx.x < 32 && i1 > i0)
+          gather_entries_warp<PAR>(p, qo, p.q[par][0], cnt0, pk0 >> 31, i0, i1, (int)L, enq, fbn, sm.spec != 0, F1);
       } else {
-        expand_bitmap<PAR>(p, sm, qo, acc, fbc, (int)L, enq, fbn, par);
+        if (q_valid) {
+          for (int bin = 2; bin >= 1; --bin) {
+            const unsigned long long pk = sm.bins[bin];
+            gather_bin<PAR>(p, sm, qo, acc, p.q[par][bin], (unsigned)(pk & kCountMask), pk >> 31, (int)L, enq, fbn);
+          }
+          gather_entries<PAR>(p, sm, qo, acc, p.q[par][0], cnt0, pk0 >> 31, (int)L, enq, fbn);
+        } else {
+          expand_bitmap<PAR>(p, sm, qo, acc, fbc, (int)L, enq, fbn, par);
+        }
+        if (enq) flush(sm, qo);
+        publish_acc(sm, acc, F1, nullptr);
       }
-      if (enq) flush(sm, qo);
-      publish_acc(sm, acc, F1, nullptr);
       if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       if (!q_valid) {
         // heavy vertices deferred by the fused sweep: expand them grid-wide
