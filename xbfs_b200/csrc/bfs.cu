@@ -316,10 +316,11 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane) {
 #pragma unroll
   for (int i = 0; i < 8; ++i) a = fmaf(W1T[i * 32 + lane], __shfl_sync(0xffffffffu, f, i), a);
   a = fmaxf(a, 0.f);
-  float b = B2[lane];
-#pragma unroll 8
-  for (int i = 0; i < 32; ++i) b = fmaf(W2T[i * 32 + lane], __shfl_sync(0xffffffffu, a, i), b);
-  b = fmaxf(b, 0.f);
+  // four independent accumulators shorten the dependent FMA chain of layer 2
+  float bq[4] = {B2[lane], 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int i = 0; i < 32; ++i) bq[i & 3] = fmaf(W2T[i * 32 + lane], __shfl_sync(0xffffffffu, a, i), bq[i & 3]);
+  const float b = fmaxf((bq[0] + bq[1]) + (bq[2] + bq[3]), 0.f);
   float o[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) o[k] = warp_sum(W3[k * 32 + lane] * b) + B3[k];

@@ -228,7 +228,9 @@ def evaluate(graph_specs: list[tuple], sources: int = 8, seed: int = 99, reps: i
 
 
 TRAIN_SET = [("rmat", 16, 16, 11), ("rmat", 18, 8, 12), ("rmat", 19, 32, 13), ("rmat", 20, 16, 14),
-             ("rmat", 21, 32, 15), ("rmat", 22, 16, 16), ("er", 200000, 8.0, 17), ("er", 2000000, 16.0, 18),
+             ("rmat", 21, 32, 15), ("rmat", 22, 16, 16), ("rmat", 20, 8, 21), ("rmat", 22, 32, 22),
+             ("er", 200000, 8.0, 17), ("er", 2000000, 16.0, 18), ("er", 1000000, 8.0, 19),
+             ("er", 3000000, 4.0, 20), ("er", 6000000, 8.0, 23),
              ("grid", 512, 512), ("grid", 1024, 256), ("grid", 2048, 1024, 1)]
 EVAL_SET = [("rmat", 23, 32, 1), ("rmat", 22, 16, 1), ("grid", 1024, 1024), ("er", 4000000, 8.0, 3)]
 
