@@ -13,8 +13,10 @@
 //    free slot and for room in an HBM budget (their output array is
 //    allocated from a stream-ordered pool when admitted).
 //  * Ticks are top-down: the frontier queue (vertex ids with exclusive edge
-//    offsets) is expanded edge-balanced across the GPU, touched vertices are
-//    merged, their new bits recorded and queued for the next tick. Graphs run
+//    offsets) is expanded edge-balanced across the GPU; each edge claims the
+//    slots its target lacks with one 64-bit atomicOr, and the first claimant
+//    of a vertex in a tick queues it for the next. A round of ticks runs in
+//    one cooperative launch with one grid barrier per tick. Graphs run
 //    on their own streams so their ticks overlap on the device; the host
 //    intervenes every K ticks (K grows with a graph's observed depth, so
 //    long-diameter graphs are not host-bound).
@@ -37,9 +39,12 @@ constexpr int kSlots = 64;
 constexpr int kRing = 64;  // ticks between host interventions, at most
 constexpr unsigned long long kCountMask = (1ull << 31) - 1;
 
+// Buffers by tick: frontier masks F[t % 3] (read at tick t, written for t+1,
+// retired at t+1), frontier queues q[t % 4] (expanded at tick t, filled at
+// t-1, their ids read again when retiring at t+1, counter reset at t-2).
 struct Ctl {
-  unsigned long long q[3];            // packed (edges << 31) | count, frontier queue ring
-  unsigned int tcount[2];             // touched-list length by tick parity
+  GridBarrier bar;                    // barrier of the round kernel (zeroed before each round)
+  unsigned long long q[4];            // packed (edges << 31) | count, frontier queue ring
   unsigned long long active[kRing];   // OR of the bits gained at each tick of the window
   unsigned long long msum[kSlots];    // per slot: sum of degrees of reached vertices
 };
@@ -49,35 +54,39 @@ struct Params {
   const int* csr;
   long long V;
   unsigned long long* vis;
-  unsigned long long* F[2];
-  unsigned long long* N;
-  uint32_t* touched;
-  int* tlist;
-  int* qids[3];
-  unsigned* qeb[3];
+  unsigned long long* F[3];
+  int* qids[4];
+  unsigned* qeb[4];
   int* const* out;     // device table: output array of each slot (or null)
   const long long* join;  // device table: join tick of each slot
   Ctl* ctl;
 };
 
-// tick t reads frontier F[t&1] and queue t%3, writes F[(t+1)&1] and queue (t+1)%3
-__global__ void __launch_bounds__(kBlock) k_sv_expand(Params p, long long t) {
+// Tick t, one phase: every edge (u, v) of frontier queue t offers u's slot
+// mask to v; the slots v did not have yet are claimed with one 64-bit
+// atomicOr on vis[v] (each slot bit is won exactly once), recorded in v's
+// output row for each won slot (level t + 1 - join), added to the next
+// frontier mask, and the thread whose OR found v's next mask empty queues v
+// for tick t+1 (so v is queued once). Edge-balanced: part takes an equal
+// share of the queue's edges.
+__device__ void sv_tick(const Params& p, long long t, unsigned nparts, unsigned part,
+                        unsigned long long* s_msum, unsigned long long* s_act) {
   __shared__ long long wbeg[kBlock + 1];
   __shared__ unsigned web[kBlock + 1];
   __shared__ int wu[kBlock + 1];
   __shared__ int next_s;
   const int lane = threadIdx.x & 31;
-  const int qs = (int)(t % 3);
+  const int qs = (int)(t % 4), qn = (int)((t + 1) % 4);
   const unsigned long long pk = ld_cg_u64(&p.ctl->q[qs]);
   const unsigned cnt = (unsigned)(pk & kCountMask);
   const unsigned long long M = pk >> 31;
-  const unsigned long long G = gridDim.x;
-  const unsigned long long lo = M * blockIdx.x / G, hi = M * (blockIdx.x + 1) / G;
+  const unsigned long long G = nparts;
+  const unsigned long long lo = M * part / G, hi = M * (part + 1) / G;
   if (cnt == 0 || lo >= hi) return;
   const int* ids = p.qids[qs];
   const unsigned* eb = p.qeb[qs];
-  const unsigned long long* Fc = p.F[t & 1];
-  unsigned* tctr = &p.ctl->tcount[t & 1];
+  const unsigned long long* Fc = p.F[t % 3];
+  unsigned long long* Fn = p.F[(t + 1) % 3];
   if (threadIdx.x < 32) {
     unsigned a = 0, b = cnt;
     while (b - a > 32) {
@@ -96,6 +105,7 @@ __global__ void __launch_bounds__(kBlock) k_sv_expand(Params p, long long t) {
   }
   __syncthreads();
   unsigned s = (unsigned)next_s;
+  unsigned long long act = 0;
   for (unsigned long long r = lo; r < hi; r += kBlock) {
     const unsigned long long rhi = (r + kBlock < hi) ? r + kBlock : hi;
     for (int i = threadIdx.x; i <= kBlock; i += kBlock) {
@@ -116,6 +126,7 @@ __global__ void __launch_bounds__(kBlock) k_sv_expand(Params p, long long t) {
     const unsigned long long e = r + threadIdx.x;
     bool first = false;
     int v = 0;
+    long long deg = 0;
     if (e < rhi) {
       int a = 0, c = kBlock + 1;
       while (c - a > 1) {
@@ -124,19 +135,38 @@ __global__ void __launch_bounds__(kBlock) k_sv_expand(Params p, long long t) {
       }
       const int u = wu[a];
       v = ld_stream_i32(p.csr + wbeg[a] + (long long)(e - web[a]));
-      const unsigned long long m = Fc[u] & ~ld_cg_u64(p.vis + v);
+      const unsigned long long m = ld_cg_u64(Fc + u) & ~ld_cg_u64(p.vis + v);
       if (m) {
-        red_or_u64(p.N + v, m);
-        const uint32_t bit = 1u << (v & 31);
-        if (!(ld_cg_u32(p.touched + (v >> 5)) & bit)) first = !(atomicOr(p.touched + (v >> 5), bit) & bit);
+        const unsigned long long gained = m & ~atomicOr(p.vis + v, m);
+        if (gained) {
+          const long long b0 = ld_nc_i64(p.beg + v);
+          deg = ld_nc_i64(p.beg + v + 1) - b0;
+          // a vertex without edges is never expanded: it gets levels, no frontier bits
+          const unsigned long long prev = deg > 0 ? atomicOr(Fn + v, gained) : ~0ull;
+          act |= gained;
+          for (unsigned long long bits = gained; bits; bits &= bits - 1) {
+            const int sl = __ffsll((long long)bits) - 1;
+            int* o = p.out[sl];
+            if (o) o[v] = (int)(t + 1 - p.join[sl]);
+            if (deg) atomicAdd(&s_msum[sl], (unsigned long long)deg);
+          }
+          first = prev == 0 && deg > 0;
+        }
       }
     }
-    const unsigned tm = __ballot_sync(0xffffffffu, first);
-    if (tm) {
-      unsigned base = 0;
-      if (lane == 0) base = atomicAdd(tctr, (unsigned)__popc(tm));
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if (first) p.tlist[base + __popc(tm & ((1u << lane) - 1))] = v;
+    // warp-aggregated append of the first claimants to queue t+1
+    const unsigned mask = __ballot_sync(0xffffffffu, first);
+    if (mask) {
+      const long long d = first ? deg : 0;
+      const long long inc = warp_inclusive_scan(d);
+      unsigned long long old = 0;
+      if (lane == 31) old = atomicAdd(&p.ctl->q[qn], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
+      old = __shfl_sync(0xffffffffu, old, 31);
+      if (first) {
+        const unsigned slot = (unsigned)(old & kCountMask) + __popc(mask & ((1u << lane) - 1));
+        p.qids[qn][slot] = v;
+        p.qeb[qn][slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - d));
+      }
     }
     if (threadIdx.x == 0 && rhi < hi) {
       int a = 0, c = kBlock + 1;
@@ -149,106 +179,66 @@ __global__ void __launch_bounds__(kBlock) k_sv_expand(Params p, long long t) {
     __syncthreads();
     s = (unsigned)next_s;
   }
+  act = __reduce_or_sync(0xffffffffu, (unsigned)act) |
+        ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(act >> 32)) << 32);
+  if (lane == 0 && act) atomicOr(s_act, act);
 }
 
-// Merge the touched vertices of tick t: new bits become visited and the next
-// frontier, each new (vertex, slot) gets its level in the slot's output, the
-// vertex is queued for tick t+1, and the tick's gained-bit mask is recorded.
-__global__ void __launch_bounds__(kBlock) k_sv_merge(Params p, long long t) {
-  __shared__ unsigned long long s_msum[kSlots];
-  __shared__ unsigned long long s_act;
-  if (threadIdx.x < kSlots) s_msum[threadIdx.x] = 0;
-  if (threadIdx.x == 0) s_act = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const unsigned tc = ld_cg_u32(&p.ctl->tcount[t & 1]);
-  const int qn = (int)((t + 1) % 3);
-  unsigned long long* Fn = p.F[(t + 1) & 1];
-  unsigned long long act = 0;
-  for (long long i0 = blockIdx.x * (long long)kBlock; i0 < tc; i0 += (long long)gridDim.x * kBlock) {
-    const long long i = i0 + threadIdx.x;
-    bool have = false;
-    int v = 0;
-    long long deg = 0;
-    if (i < tc) {
-      v = p.tlist[i];
-      p.touched[v >> 5] = 0u;
-      const unsigned long long a = p.N[v];
-      p.N[v] = 0ull;
-      const unsigned long long vv = p.vis[v];
-      const unsigned long long nw = a & ~vv;
-      if (nw) {
-        p.vis[v] = vv | nw;
-        Fn[v] = nw;
-        act |= nw;
-        const long long b0 = ld_nc_i64(p.beg + v);
-        deg = ld_nc_i64(p.beg + v + 1) - b0;
-        unsigned long long bits = nw;
-        while (bits) {
-          const int s = __ffsll((long long)bits) - 1;
-          bits &= bits - 1;
-          int* o = p.out[s];
-          if (o) o[v] = (int)(t + 1 - p.join[s]);
-          if (deg) atomicAdd(&s_msum[s], (unsigned long long)deg);
-        }
-        have = deg > 0;
-      }
-    }
-    // warp-aggregated append to queue t+1
-    const unsigned mask = __ballot_sync(0xffffffffu, have);
-    if (mask) {
-      long long d = have ? deg : 0;
-      const long long inc = warp_inclusive_scan(d);
-      unsigned long long old = 0;
-      if (lane == 31) old = atomicAdd(&p.ctl->q[qn], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
-      old = __shfl_sync(0xffffffffu, old, 31);
-      if (have) {
-        const unsigned slot = (unsigned)(old & kCountMask) + __popc(mask & ((1u << lane) - 1));
-        p.qids[qn][slot] = v;
-        p.qeb[qn][slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - d));
-      }
-    }
-  }
-  act = __reduce_or_sync(0xffffffffu, (unsigned)act) | ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(act >> 32)) << 32);
-  if (lane == 0 && act) atomicOr(&s_act, act);
-  __syncthreads();
-  if (threadIdx.x < kSlots && s_msum[threadIdx.x]) atomicAdd(&p.ctl->msum[threadIdx.x], s_msum[threadIdx.x]);
-  if (threadIdx.x == 0 && s_act) atomicOr(&p.ctl->active[t % kRing], s_act);
-}
-
-// Retire frontier t (clear its F entries) and reset the counters tick t+1
-// does not use any more.
-__global__ void k_sv_retire(Params p, long long t) {
-  const int qs = (int)(t % 3);
+// Clears the frontier masks of tick t (the vertices of queue t).
+__device__ void sv_retire(const Params& p, long long t, unsigned nparts, unsigned part) {
+  const int qs = (int)(t % 4);
   const unsigned cnt = (unsigned)(ld_cg_u64(&p.ctl->q[qs]) & kCountMask);
-  unsigned long long* Fc = p.F[t & 1];
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x)
+  unsigned long long* Fc = p.F[t % 3];
+  for (long long i = part * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)nparts * blockDim.x)
     Fc[p.qids[qs][i]] = 0ull;
 }
 
-__global__ void k_sv_reset(Params p, long long t) {
-  // before tick t: queue (t+1)%3 empty, touched counter of t empty, active slot of t empty
-  if (threadIdx.x == 0) {
-    p.ctl->q[(t + 1) % 3] = 0ull;
-    p.ctl->tcount[t & 1] = 0u;
-    p.ctl->active[t % kRing] = 0ull;
+// One round of k ticks from t0 in one cooperative launch, one grid barrier
+// per tick. During tick t the blocks also retire frontier t-1 (its mask
+// buffer is neither read nor written at tick t) and block 0 resets the
+// queue counter of tick t+2 (last used at tick t-2) and, inside the round,
+// the activity word of tick t+1. Every wait is bounded
+// (XBFS_ERR_DEVICE_TIMEOUT).
+__global__ void __launch_bounds__(kBlock) k_sv_round(Params p, long long t0, int k, unsigned long long timeout_ns) {
+  __shared__ unsigned long long s_msum[kSlots];
+  __shared__ unsigned long long s_act;
+  const unsigned G = gridDim.x, b = blockIdx.x;
+  uint32_t epoch = 0;
+  for (int i = 0; i < k; ++i) {
+    const long long t = t0 + i;
+    if (threadIdx.x < kSlots) s_msum[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s_act = 0;
+    if (b == 0 && threadIdx.x == 0) {
+      p.ctl->q[(t + 2) % 4] = 0ull;
+      // the first tick's activity word is zeroed by the host before the round
+      if (i + 1 < k) p.ctl->active[(t + 1) % kRing] = 0ull;
+    }
+    __syncthreads();
+    if (t > 0) sv_retire(p, t - 1, G, b);
+    sv_tick(p, t, G, b, s_msum, &s_act);
+    __syncthreads();
+    if (threadIdx.x < kSlots && s_msum[threadIdx.x]) atomicAdd(&p.ctl->msum[threadIdx.x], s_msum[threadIdx.x]);
+    if (threadIdx.x == 0 && s_act) atomicOr(&p.ctl->active[t % kRing], s_act);
+    if (!grid_sync(&p.ctl->bar, G, epoch, timeout_ns)) return;
   }
 }
 
-// Seed slot s at src for tick t (its frontier bit, its level 0, a queue entry).
+// Seed slot s at src for tick t (its visited and frontier bit, level 0, a
+// queue entry).
 __global__ void k_sv_seed(Params p, long long t, int s, int src) {
   if (threadIdx.x != 0) return;
   const unsigned long long bit = 1ull << s;
   p.vis[src] |= bit;
-  p.F[t & 1][src] |= bit;
   if (p.out[s]) p.out[s][src] = 0;
-  p.ctl->msum[s] = 0;
   const long long b0 = p.beg[src], d = p.beg[src + 1] - b0;
   p.ctl->msum[s] = (unsigned long long)d;
-  if (d > 0) {
-    const unsigned long long old = atomicAdd(&p.ctl->q[t % 3], ((unsigned long long)d << 31) | 1ull);
-    p.qids[t % 3][old & kCountMask] = src;
-    p.qeb[t % 3][old & kCountMask] = (unsigned)(old >> 31);
+  if (d == 0) return;  // nothing to expand: the request completes at its first tick
+  const unsigned long long prev = p.F[t % 3][src];
+  p.F[t % 3][src] = prev | bit;
+  if (prev == 0) {  // queued once per tick, whatever the number of slots seeded there
+    const unsigned long long old = atomicAdd(&p.ctl->q[t % 4], ((unsigned long long)d << 31) | 1ull);
+    p.qids[t % 4][old & kCountMask] = src;
+    p.qeb[t % 4][old & kCountMask] = (unsigned)(old >> 31);
   }
 }
 
@@ -277,7 +267,7 @@ struct ServeRequest {
 struct SlotBatch {
   Graph* g = nullptr;
   cudaStream_t stream = nullptr;
-  DevBuf vis, F0, F1, N, touched, tlist, q[3], qe[3], ctl, out_tab, join_tab;
+  DevBuf vis, F[3], q[4], qe[4], ctl, out_tab, join_tab;
   sv::Params p;
   long long tick = 0;
   int req_of_slot[sv::kSlots];
@@ -285,6 +275,7 @@ struct SlotBatch {
   std::deque<int> waiting;
   int k_ticks = 1;
   int grid = 0;
+  int max_coop = 0;              // blocks of k_sv_round that can be resident at once
   bool inflight = false;         // a round of ticks is on the stream
   int round_k = 0;               // its length
   long long issued = 0;          // first tick not yet issued
@@ -311,21 +302,19 @@ struct Server {
 
 static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
   b.g = g;
-  const long long V = g->V, nw = (V + 31) / 32 + 64;
+  const long long V = g->V;
   xbfs_status st;
-  if ((st = b.vis.ensure(V * 8)) || (st = b.F0.ensure(V * 8)) || (st = b.F1.ensure(V * 8)) || (st = b.N.ensure(V * 8)) ||
-      (st = b.touched.ensure(nw * 4)) || (st = b.tlist.ensure(V * 4 + 4)) || (st = b.ctl.ensure(sizeof(sv::Ctl))) ||
+  if ((st = b.vis.ensure(V * 8)) || (st = b.ctl.ensure(sizeof(sv::Ctl))) ||
       (st = b.out_tab.ensure(sizeof(int*) * sv::kSlots)) || (st = b.join_tab.ensure(8 * sv::kSlots)))
     return st;
-  // a tick's queue holds at most V merged vertices plus the seeds of one round
   for (int i = 0; i < 3; ++i)
+    if ((st = b.F[i].ensure(V * 8))) return st;
+  // a tick queues each vertex at most once, plus the seeds of one round
+  for (int i = 0; i < 4; ++i)
     if ((st = b.q[i].ensure((V + sv::kSlots + 1) * 4)) || (st = b.qe[i].ensure((V + sv::kSlots + 1) * 4))) return st;
   XBFS_CUDA_TRY(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
   XBFS_CUDA_TRY(cudaMemsetAsync(b.vis.p, 0, V * 8, b.stream));
-  XBFS_CUDA_TRY(cudaMemsetAsync(b.F0.p, 0, V * 8, b.stream));
-  XBFS_CUDA_TRY(cudaMemsetAsync(b.F1.p, 0, V * 8, b.stream));
-  XBFS_CUDA_TRY(cudaMemsetAsync(b.N.p, 0, V * 8, b.stream));
-  XBFS_CUDA_TRY(cudaMemsetAsync(b.touched.p, 0, nw * 4, b.stream));
+  for (int i = 0; i < 3; ++i) XBFS_CUDA_TRY(cudaMemsetAsync(b.F[i].p, 0, V * 8, b.stream));
   XBFS_CUDA_TRY(cudaMemsetAsync(b.ctl.p, 0, sizeof(sv::Ctl), b.stream));
   XBFS_CUDA_TRY(cudaMemsetAsync(b.out_tab.p, 0, sizeof(int*) * sv::kSlots, b.stream));
   XBFS_CUDA_TRY(cudaMemsetAsync(b.join_tab.p, 0, 8 * sv::kSlots, b.stream));
@@ -334,12 +323,8 @@ static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
   p.csr = g->csr.as<int>();
   p.V = V;
   p.vis = b.vis.as<unsigned long long>();
-  p.F[0] = b.F0.as<unsigned long long>();
-  p.F[1] = b.F1.as<unsigned long long>();
-  p.N = b.N.as<unsigned long long>();
-  p.touched = b.touched.as<uint32_t>();
-  p.tlist = b.tlist.as<int>();
-  for (int i = 0; i < 3; ++i) {
+  for (int i = 0; i < 3; ++i) p.F[i] = b.F[i].as<unsigned long long>();
+  for (int i = 0; i < 4; ++i) {
     p.qids[i] = b.q[i].as<int>();
     p.qeb[i] = b.qe[i].as<unsigned>();
   }
@@ -347,7 +332,11 @@ static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
   p.join = b.join_tab.as<long long>();
   p.ctl = b.ctl.as<sv::Ctl>();
   for (int s = 0; s < sv::kSlots; ++s) b.req_of_slot[s] = -1;
-  b.grid = nsm * 4;
+  int per_sm = 0;
+  XBFS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)sv::k_sv_round, sv::kBlock, 0));
+  if (per_sm < 1) return set_error(XBFS_ERR_INTERNAL, "serving round kernel cannot be resident");
+  b.max_coop = nsm * per_sm;
+  b.grid = b.max_coop;
   return XBFS_OK;
 }
 
@@ -355,14 +344,15 @@ static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
 // (sized by the caller from the frontier; the kernels are grid-stride, so a
 // frontier that outgrows it is still covered).
 static xbfs_status batch_ticks(SlotBatch& b, int k, int grid) {
-  for (int i = 0; i < k; ++i) {
-    const long long t = b.tick + i;
-    sv::k_sv_reset<<<1, 32, 0, b.stream>>>(b.p, t);
-    sv::k_sv_expand<<<grid, sv::kBlock, 0, b.stream>>>(b.p, t);
-    sv::k_sv_merge<<<grid, sv::kBlock, 0, b.stream>>>(b.p, t);
-    sv::k_sv_retire<<<grid, 256, 0, b.stream>>>(b.p, t);
-  }
-  XBFS_CUDA_TRY(cudaGetLastError());
+  if (grid > b.max_coop) grid = b.max_coop;
+  sv::Ctl* c = b.ctl.as<sv::Ctl>();
+  XBFS_CUDA_TRY(cudaMemsetAsync(&c->bar, 0, sizeof(GridBarrier), b.stream));
+  XBFS_CUDA_TRY(cudaMemsetAsync(&c->active[b.tick % sv::kRing], 0, 8, b.stream));
+  long long t0 = b.tick;
+  unsigned long long timeout_ns = 10ull * 1000 * 1000 * 1000;
+  void* args[] = {&b.p, &t0, &k, &timeout_ns};
+  XBFS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)sv::k_sv_round, dim3(grid), dim3(sv::kBlock), args, 0,
+                                            b.stream));
   return XBFS_OK;
 }
 
@@ -474,6 +464,9 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
       if (q == cudaErrorNotReady) continue;
       XBFS_CUDA_TRY(q);
       b.inflight = false;
+      if (hctl[gi].bar.err != 0)
+        return set_error((xbfs_status)hctl[gi].bar.err, "serving round on graph %d reported %s", gi,
+                         xbfs_strerror(hctl[gi].bar.err));
       const int k = b.round_k;
       unsigned long long finished = 0;
       for (int i = 0; i < k; ++i) {
@@ -559,12 +552,15 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
       if (!b.busy) continue;
       ++running;
       const int k = std::max(1, std::min(b.k_ticks, sv::kRing - (int)(b.tick % sv::kRing)));
-      // Blocks per tick kernel from the frontier the round starts with (4x
-      // headroom for growth inside the round): small frontiers (grids) use a
-      // few SMs, so the batches' streams share the GPU instead of taking turns.
+      // Blocks of the round from the frontier it starts with (4x headroom for
+      // growth inside the round) when the rounds are long, i.e. the graph's
+      // traversals are deep and their frontiers grow slowly: those batches
+      // then use a few SMs and share the GPU instead of taking turns. Short
+      // rounds (low-diameter graphs, whose frontier can grow a thousandfold
+      // in one tick) get every resident block.
       int grid = b.grid;
-      if (b.tick > 0) {
-        const unsigned long long pk = hctl[gi].q[b.tick % 3];
+      if (b.tick > 0 && k >= 16) {  // long rounds: the frontier grows slowly (long-diameter graphs)
+        const unsigned long long pk = hctl[gi].q[b.tick % 4];
         const unsigned long long work = std::max<unsigned long long>(pk >> 31, pk & sv::kCountMask);
         const unsigned long long want = (work * 4 + sv::kBlock * 2 - 1) / (sv::kBlock * 2);
         grid = (int)std::min<unsigned long long>((unsigned long long)b.grid, std::max<unsigned long long>(8, want));
