@@ -510,15 +510,28 @@ def extra_serve(args):
     srv = Server(graphs)
     res = {"graphs": ["rmat-s%d-ef16" % sp[1] if sp[0] == "rmat" else "grid-%dx%d" % sp[1:] for sp in specs], "rates": []}
     rng = np.random.default_rng(args.seed)
+    is_grid = np.array([sp[0] == "grid" for sp in specs])
     for rate in (1e2, 1e3, 1e4, 1e5):
+        # two independent traces per rate; latencies pooled (a single trace of
+        # a few hundred requests over 8 very different graphs is noisy)
         n = int(min(400, max(40, rate * 2)))
-        gid = rng.integers(0, len(graphs), size=n).astype(np.int32)
-        src = np.array([pick_sources(begs[gi], 1, int(rate) + i)[0] for i, gi in enumerate(gid)], dtype=np.int32)
-        arr = np.cumsum(rng.exponential(1e6 / rate, size=n))
-        r = srv.run(gid, src, arr, keep_outputs=False)
-        res["rates"].append({"rate_per_s": rate, "requests": n, "p50_ms": round(r["p50_us"] / 1e3, 3),
-                             "p99_ms": round(r["p99_us"] / 1e3, 3), "gteps": round(r["gteps"], 3),
-                             "wall_s": round(r["wall_us"] / 1e6, 3)})
+        lat, kinds, mc, wall = [], [], 0, 0.0
+        for rep in range(2):
+            gid = rng.integers(0, len(graphs), size=n).astype(np.int32)
+            src = np.array([pick_sources(begs[gi], 1, int(rate) + 1000 * rep + i)[0] for i, gi in enumerate(gid)],
+                           dtype=np.int32)
+            arr = np.cumsum(rng.exponential(1e6 / rate, size=n))
+            r = srv.run(gid, src, arr, keep_outputs=False)
+            lat.append(r["latency_us"])
+            kinds.append(is_grid[gid])
+            mc += int(r["edges_mc"].sum())
+            wall += r["wall_us"]
+        lat, kinds = np.concatenate(lat) / 1e3, np.concatenate(kinds)
+        pct = lambda a, q: round(float(np.percentile(a, q)), 3) if len(a) else None
+        res["rates"].append({"rate_per_s": rate, "requests": 2 * n, "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+                             "rmat_p50_ms": pct(lat[~kinds], 50), "rmat_p99_ms": pct(lat[~kinds], 99),
+                             "grid_p50_ms": pct(lat[kinds], 50), "grid_p99_ms": pct(lat[kinds], 99),
+                             "gteps": round(mc / (wall * 1e-6) / 1e9, 3), "wall_s": round(wall / 1e6, 3)})
     srv.free()
     for g in graphs:
         g.free()

@@ -86,3 +86,26 @@ def test_run_without_keeping_outputs_reports_edges():
     for i, (g, s) in enumerate(zip(gid, src)):
         assert res["edges_mc"][i] == oracle.edges_mc(cpu[g][0], oracle.bfs_queue(cpu[g][0], cpu[g][1], int(s)))
     assert res["p99_us"] >= res["p50_us"] > 0
+
+
+def test_directed_graph_and_isolated_sources():
+    """A directed CSR (bottom-up ticks are invalid there and must stay off), a
+    directed R-MAT-like graph and sources without edges: every answer equals
+    the oracle's."""
+    from tests.conftest import hand_graphs
+    hg = hand_graphs()
+    beg, csr = gen_rmat_host(12, 16, 7)
+    # drop the reverse of every third edge to make it directed
+    keep = np.ones(len(csr), dtype=bool)
+    src_of = np.repeat(np.arange(len(beg) - 1), np.diff(beg))
+    keep[(src_of > csr) & (np.arange(len(csr)) % 3 == 0)] = False
+    dbeg = np.concatenate([[0], np.cumsum(np.bincount(src_of[keep], minlength=len(beg) - 1))]).astype(np.int64)
+    dcsr = csr[keep].astype(np.int32)
+    cpu = [hg["directed_chain"], (dbeg, dcsr), hg["isolated_src"]]
+    graphs = [Graph.from_csr(b, c) for b, c in cpu]
+    gid = np.array([0, 1, 1, 2, 2, 1, 0], dtype=np.int32)
+    src = np.array([0, 5, 17, 0, 1, 100, 3], dtype=np.int32)
+    srv = Server(graphs)
+    res = srv.run(gid, src, np.zeros(len(gid)), to_host=True)
+    for i, (g, s) in enumerate(zip(gid, src)):
+        assert np.array_equal(res["levels"][i], oracle.bfs_queue(cpu[g][0], cpu[g][1], int(s))), i

@@ -52,7 +52,8 @@ struct Ctl {
 struct Params {
   const long long* beg;
   const int* csr;
-  long long V;
+  long long V, E;
+  int allow_bu;        // symmetric CSR: bottom-up ticks are valid
   unsigned long long* vis;
   unsigned long long* F[3];
   int* qids[4];
@@ -184,6 +185,65 @@ __device__ void sv_tick(const Params& p, long long t, unsigned nparts, unsigned 
   if (lane == 0 && act) atomicOr(s_act, act);
 }
 
+// Bottom-up tick t, for large frontiers: every vertex still lacking some of
+// the running slots probes its neighbours' frontier masks until it has found
+// all of them or runs out of neighbours. Each vertex is handled by exactly one
+// thread, so visited, next-frontier mask and queue entry are plain writes.
+// Blocks take contiguous vertex ranges.
+__device__ void sv_tick_bu(const Params& p, long long t, unsigned long long running, unsigned nparts,
+                           unsigned part, unsigned long long* s_msum, unsigned long long* s_act) {
+  const int lane = threadIdx.x & 31;
+  const int qn = (int)((t + 1) % 4);
+  const unsigned long long* Fc = p.F[t % 3];
+  unsigned long long* Fn = p.F[(t + 1) % 3];
+  const long long per = (p.V + nparts - 1) / nparts;
+  const long long v0 = per * part, v1 = (v0 + per < p.V) ? v0 + per : p.V;
+  unsigned long long act = 0;
+  for (long long base = v0; base < v1; base += blockDim.x) {
+    const long long v = base + threadIdx.x;
+    bool have = false;
+    long long deg = 0;
+    if (v < v1) {
+      const unsigned long long vv = ld_cg_u64(p.vis + v);
+      const unsigned long long needed = running & ~vv;
+      if (needed) {
+        const long long b0 = ld_nc_i64(p.beg + v), b1 = ld_nc_i64(p.beg + v + 1);
+        unsigned long long got = 0;
+        for (long long e = b0; e < b1 && got != needed; ++e) got |= ld_cg_u64(Fc + ld_stream_i32(p.csr + e)) & needed;
+        if (got) {
+          deg = b1 - b0;
+          p.vis[v] = vv | got;
+          Fn[v] = got;
+          act |= got;
+          for (unsigned long long bits = got; bits; bits &= bits - 1) {
+            const int sl = __ffsll((long long)bits) - 1;
+            int* o = p.out[sl];
+            if (o) o[v] = (int)(t + 1 - p.join[sl]);
+            atomicAdd(&s_msum[sl], (unsigned long long)deg);
+          }
+          have = true;
+        }
+      }
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, have);
+    if (mask) {
+      const long long d = have ? deg : 0;
+      const long long inc = warp_inclusive_scan(d);
+      unsigned long long old = 0;
+      if (lane == 31) old = atomicAdd(&p.ctl->q[qn], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
+      old = __shfl_sync(0xffffffffu, old, 31);
+      if (have) {
+        const unsigned slot = (unsigned)(old & kCountMask) + __popc(mask & ((1u << lane) - 1));
+        p.qids[qn][slot] = (int)v;
+        p.qeb[qn][slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - d));
+      }
+    }
+  }
+  act = __reduce_or_sync(0xffffffffu, (unsigned)act) |
+        ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(act >> 32)) << 32);
+  if (lane == 0 && act) atomicOr(s_act, act);
+}
+
 // Clears the frontier masks of tick t (the vertices of queue t).
 __device__ void sv_retire(const Params& p, long long t, unsigned nparts, unsigned part) {
   const int qs = (int)(t % 4);
@@ -199,7 +259,13 @@ __device__ void sv_retire(const Params& p, long long t, unsigned nparts, unsigne
 // queue counter of tick t+2 (last used at tick t-2) and, inside the round,
 // the activity word of tick t+1. Every wait is bounded
 // (XBFS_ERR_DEVICE_TIMEOUT).
-__global__ void __launch_bounds__(kBlock) k_sv_round(Params p, long long t0, int k, unsigned long long timeout_ns) {
+// A tick runs bottom-up when its frontier's edges exceed E / kBuRatio (the
+// frontier queue's packed counter is final after the previous barrier, so
+// every block takes the same decision); `running` = the slots in the batch.
+constexpr long long kBuRatio = 8;
+
+__global__ void __launch_bounds__(kBlock) k_sv_round(Params p, long long t0, int k, unsigned long long timeout_ns,
+                                                     unsigned long long running) {
   __shared__ unsigned long long s_msum[kSlots];
   __shared__ unsigned long long s_act;
   const unsigned G = gridDim.x, b = blockIdx.x;
@@ -215,7 +281,11 @@ __global__ void __launch_bounds__(kBlock) k_sv_round(Params p, long long t0, int
     }
     __syncthreads();
     if (t > 0) sv_retire(p, t - 1, G, b);
-    sv_tick(p, t, G, b, s_msum, &s_act);
+    const unsigned long long qk = ld_cg_u64(&p.ctl->q[t % 4]);
+    if (p.allow_bu && (long long)(qk >> 31) * kBuRatio > p.E)
+      sv_tick_bu(p, t, running, G, b, s_msum, &s_act);
+    else
+      sv_tick(p, t, G, b, s_msum, &s_act);
     __syncthreads();
     if (threadIdx.x < kSlots && s_msum[threadIdx.x]) atomicAdd(&p.ctl->msum[threadIdx.x], s_msum[threadIdx.x]);
     if (threadIdx.x == 0 && s_act) atomicOr(&p.ctl->active[t % kRing], s_act);
@@ -322,6 +392,8 @@ static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
   p.beg = g->beg.as<long long>();
   p.csr = g->csr.as<int>();
   p.V = V;
+  p.E = g->E;
+  p.allow_bu = g->symmetric ? 1 : 0;
   p.vis = b.vis.as<unsigned long long>();
   for (int i = 0; i < 3; ++i) p.F[i] = b.F[i].as<unsigned long long>();
   for (int i = 0; i < 4; ++i) {
@@ -350,7 +422,8 @@ static xbfs_status batch_ticks(SlotBatch& b, int k, int grid) {
   XBFS_CUDA_TRY(cudaMemsetAsync(&c->active[b.tick % sv::kRing], 0, 8, b.stream));
   long long t0 = b.tick;
   unsigned long long timeout_ns = 10ull * 1000 * 1000 * 1000;
-  void* args[] = {&b.p, &t0, &k, &timeout_ns};
+  unsigned long long running = b.busy;
+  void* args[] = {&b.p, &t0, &k, &timeout_ns, &running};
   XBFS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)sv::k_sv_round, dim3(grid), dim3(sv::kBlock), args, 0,
                                             b.stream));
   return XBFS_OK;
@@ -541,7 +614,12 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
         sv::k_sv_seed<<<1, 32, 0, b.stream>>>(b.p, b.issued, sl, r.src);
       }
     }
-    // issue the next round of every idle batch with running slots
+    // issue the next round of every idle batch with running slots; the
+    // resident-block budget of the device is split between the batches that
+    // have work, so that their cooperative rounds can be resident together
+    // (a round needing the whole device would wait for every other to end)
+    int with_work = 0;
+    for (int gi = 0; gi < nb; ++gi) with_work += srv->batches[gi]->busy ? 1 : 0;
     int running = 0;
     for (int gi = 0; gi < nb; ++gi) {
       SlotBatch& b = *srv->batches[gi];
@@ -565,6 +643,7 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
         const unsigned long long want = (work * 4 + sv::kBlock * 2 - 1) / (sv::kBlock * 2);
         grid = (int)std::min<unsigned long long>((unsigned long long)b.grid, std::max<unsigned long long>(8, want));
       }
+      grid = std::min(grid, std::max(8, b.max_coop / std::max(1, with_work)));
       xbfs_status st = batch_ticks(b, k, grid);
       if (st) return st;
       XBFS_CUDA_TRY(cudaMemcpyAsync(&hctl[gi], b.ctl.p, sizeof(sv::Ctl), cudaMemcpyDeviceToHost, b.stream));
