@@ -211,7 +211,7 @@ xbfs_status xbfs_bfs_noalloc(xbfs_graph* g, int32_t src, int32_t* levels, int32_
  * host or device). Sources are traversed 64 per uint64 word, up to 8 words
  * (512 sources) per pass. No counterpart in the reference (one source per
  * process). opts.policy FORCED with forced[0] = XBFS_TD_QUEUE / XBFS_BU pins
- * the direction; otherwise opts.alpha (default 4 when <= 0.5) sets the
+ * the direction; otherwise opts.alpha (default 2 when <= 0.5) sets the
  * top-down/bottom-up switch on frontier vs unfinished edges. */
 xbfs_status xbfs_bfs_batch(xbfs_graph* g, const int32_t* srcs, int32_t n, int32_t* levels,
                            const xbfs_opts* opts, xbfs_stats* stats);
