@@ -201,6 +201,8 @@ struct __align__(16) Smem {
   long long red[kBlock / 32 + 1];
   long long red4[4 * (kBlock / 32)];
   float mlp_raw[8];             // statistics the learned switch's features come from
+  float mlp_cache_f[8];         // features of its last evaluation
+  int mlp_cache_dec;            // and its decision (-1: none yet)
   LoopState ls;
   float mlp_w[1464];            // the learned switch's weights (XBFS_POLICY_MLP); must stay last
 };
@@ -295,7 +297,15 @@ __device__ void mlp_stage(const float* __restrict__ w, float* sw) {
 // strategy; log growth of the frontier; log1p of its mean degree), one per
 // lane, then the three layers with the hidden activations passed by shuffles.
 // Called by one full warp.
-__device__ int mlp_decide(const float* sw, const float* raw, int lane) {
+// Inference cache (per CTA, in shared memory): when every normalised feature
+// is within kMlpReuse of the ones the network last saw, that decision is
+// reused. Long runs of nearly identical levels (a grid's ring of a few
+// thousand vertices growing by a few per level) then skip the layers;
+// levels where the frontier changes by more than a few percent always
+// evaluate the network.
+constexpr float kMlpReuse = 0.02f;
+
+__device__ int mlp_decide(const float* sw, const float* raw, int lane, float* cache_f, int* cache_dec) {
   const float* mean = sw;
   const float* sd = sw + 8;
   const float* W1T = sw + 16;
@@ -312,6 +322,8 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane) {
     else f = log1pf(r > 0.f ? r : 0.f);
     f = (f - mean[lane]) / sd[lane];
   }
+  const bool near = lane >= 8 || fabsf(f - cache_f[lane]) < kMlpReuse;
+  if (__all_sync(0xffffffffu, near) && *cache_dec >= 0) return *cache_dec;
   float a = B1[lane];
 #pragma unroll
   for (int i = 0; i < 8; ++i) a = fmaf(W1T[i * 32 + lane], __shfl_sync(0xffffffffu, f, i), a);
@@ -327,6 +339,10 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane) {
   int best = 0;
   if (o[1] > o[best]) best = 1;
   if (o[2] > o[best]) best = 2;
+  __syncwarp();
+  if (lane < 8) cache_f[lane] = f;
+  if (lane == 0) *cache_dec = best;
+  __syncwarp();
   return best;
 }
 
@@ -1083,6 +1099,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
   if (p.absent_block > 0 && (int)blockIdx.x == p.absent_block - 1) return;  // test hook: never arrives
   if (threadIdx.x < 3) sm.cnt[threadIdx.x] = 0;
   if (p.policy == XBFS_POLICY_MLP && p.mlp) mlp_stage(p.mlp, sm.mlp_w);
+  if (threadIdx.x == 0) sm.mlp_cache_dec = -1;
   __syncthreads();
 
   // Policy state and running sums live in shared memory, owned by thread 0:
@@ -1221,7 +1238,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       // the learned switch: warp 0 evaluates it while the block waits (one
       // warp keeps the shared-memory and shuffle traffic of the network small)
       if (threadIdx.x < 32) {
-        int s2 = p.mlp ? mlp_decide(sm.mlp_w, sm.mlp_raw, threadIdx.x) : XBFS_TD_QUEUE;
+        int s2 = p.mlp ? mlp_decide(sm.mlp_w, sm.mlp_raw, threadIdx.x, sm.mlp_cache_f, &sm.mlp_cache_dec)
+                       : XBFS_TD_QUEUE;
         if (s2 == XBFS_BU && !p.allow_bu) s2 = XBFS_TD_QUEUE;
         if (threadIdx.x == 0) sm.strategy = s2;
       }

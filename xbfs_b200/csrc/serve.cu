@@ -58,10 +58,52 @@ struct Params {
   unsigned long long* F[3];
   int* qids[4];
   unsigned* qeb[4];
+  long long* qbg[4];   // CSR offset of each queued vertex
   int* const* out;     // device table: output array of each slot (or null)
   const long long* join;  // device table: join tick of each slot
   Ctl* ctl;
 };
+
+// Claim step of one edge (u, v) at tick t (see sv_tick); returns whether
+// this thread queues v for tick t+1, with v's degree and CSR offset.
+__device__ __forceinline__ bool sv_claim(const Params& p, long long t, const unsigned long long* Fc,
+                                         unsigned long long* Fn, int u, int v, long long& deg, long long& b0,
+                                         unsigned long long& act, unsigned long long* s_msum) {
+  const unsigned long long m = ld_cg_u64(Fc + u) & ~ld_cg_u64(p.vis + v);
+  if (!m) return false;
+  const unsigned long long gained = m & ~atomicOr(p.vis + v, m);
+  if (!gained) return false;
+  b0 = ld_nc_i64(p.beg + v);
+  deg = ld_nc_i64(p.beg + v + 1) - b0;
+  // a vertex without edges is never expanded: it gets levels, no frontier bits
+  const unsigned long long prev = deg > 0 ? atomicOr(Fn + v, gained) : ~0ull;
+  act |= gained;
+  for (unsigned long long bits = gained; bits; bits &= bits - 1) {
+    const int sl = __ffsll((long long)bits) - 1;
+    int* o = p.out[sl];
+    if (o) o[v] = (int)(t + 1 - p.join[sl]);
+    if (deg) atomicAdd(&s_msum[sl], (unsigned long long)deg);
+  }
+  return prev == 0 && deg > 0;
+}
+
+// Warp-aggregated append of the lanes with `have` to queue qn (full warp).
+__device__ __forceinline__ void sv_enqueue(const Params& p, int qn, bool have, int v, long long deg, long long b0) {
+  const int lane = threadIdx.x & 31;
+  const unsigned mask = __ballot_sync(0xffffffffu, have);
+  if (!mask) return;
+  const long long d = have ? deg : 0;
+  const long long inc = warp_inclusive_scan(d);
+  unsigned long long old = 0;
+  if (lane == 31) old = atomicAdd(&p.ctl->q[qn], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
+  old = __shfl_sync(0xffffffffu, old, 31);
+  if (have) {
+    const unsigned slot = (unsigned)(old & kCountMask) + __popc(mask & ((1u << lane) - 1));
+    p.qids[qn][slot] = v;
+    p.qeb[qn][slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - d));
+    p.qbg[qn][slot] = b0;
+  }
+}
 
 // Tick t, one phase: every edge (u, v) of frontier queue t offers u's slot
 // mask to v; the slots v did not have yet are claimed with one 64-bit
@@ -83,11 +125,46 @@ __device__ void sv_tick(const Params& p, long long t, unsigned nparts, unsigned 
   const unsigned long long M = pk >> 31;
   const unsigned long long G = nparts;
   const unsigned long long lo = M * part / G, hi = M * (part + 1) / G;
-  if (cnt == 0 || lo >= hi) return;
+  if (cnt == 0) return;
   const int* ids = p.qids[qs];
   const unsigned* eb = p.qeb[qs];
+  const long long* bgs = p.qbg[qs];
   const unsigned long long* Fc = p.F[t % 3];
   unsigned long long* Fn = p.F[(t + 1) % 3];
+  unsigned long long act = 0;
+  if ((unsigned long long)cnt <= 32ull * G && M <= 32ull * cnt) {
+    // small queue of low-degree vertices: each part takes an equal share of
+    // the entries (at most 32), so no part searches the queue for its start
+    const unsigned i0 = (unsigned)((unsigned long long)cnt * part / G);
+    const unsigned i1 = (unsigned)((unsigned long long)cnt * (part + 1) / G);
+    if (i0 >= i1) return;
+    const int n = (int)(i1 - i0);
+    const unsigned base = eb[i0];
+    const unsigned long long T = ((i1 < cnt) ? (unsigned long long)eb[i1] : M) - base;
+    if (threadIdx.x < n) {
+      const unsigned slot = i0 + threadIdx.x;
+      wu[threadIdx.x] = ids[slot];
+      wbeg[threadIdx.x] = bgs[slot];
+      web[threadIdx.x] = eb[slot] - base;
+    }
+    __syncthreads();
+    for (unsigned long long e0 = 0; e0 < T; e0 += kBlock) {
+      const unsigned long long e = e0 + threadIdx.x;
+      bool first = false;
+      int v = 0;
+      long long deg = 0, b0 = 0;
+      if (e < T) {
+        int a = 0, c = n;
+        while (c - a > 1) {
+          const int mid = (a + c) >> 1;
+          if ((unsigned long long)web[mid] <= e) a = mid; else c = mid;
+        }
+        v = ld_stream_i32(p.csr + wbeg[a] + (long long)(e - web[a]));
+        first = sv_claim(p, t, Fc, Fn, wu[a], v, deg, b0, act, s_msum);
+      }
+      sv_enqueue(p, qn, first, v, deg, b0);
+    }
+  } else if (lo < hi) {
   if (threadIdx.x < 32) {
     unsigned a = 0, b = cnt;
     while (b - a > 32) {
@@ -106,7 +183,6 @@ __device__ void sv_tick(const Params& p, long long t, unsigned nparts, unsigned 
   }
   __syncthreads();
   unsigned s = (unsigned)next_s;
-  unsigned long long act = 0;
   for (unsigned long long r = lo; r < hi; r += kBlock) {
     const unsigned long long rhi = (r + kBlock < hi) ? r + kBlock : hi;
     for (int i = threadIdx.x; i <= kBlock; i += kBlock) {
@@ -116,9 +192,8 @@ __device__ void sv_tick(const Params& p, long long t, unsigned nparts, unsigned 
         const unsigned x = eb[slot];
         if ((unsigned long long)x < rhi) {
           e0 = x;
-          const int u = ids[slot];
-          wu[i] = u;
-          wbeg[i] = ld_nc_i64(p.beg + u);
+          wu[i] = ids[slot];
+          wbeg[i] = bgs[slot];
         }
       }
       web[i] = e0;
@@ -127,48 +202,17 @@ __device__ void sv_tick(const Params& p, long long t, unsigned nparts, unsigned 
     const unsigned long long e = r + threadIdx.x;
     bool first = false;
     int v = 0;
-    long long deg = 0;
+    long long deg = 0, b0 = 0;
     if (e < rhi) {
       int a = 0, c = kBlock + 1;
       while (c - a > 1) {
         const int mid = (a + c) >> 1;
         if ((unsigned long long)web[mid] <= e) a = mid; else c = mid;
       }
-      const int u = wu[a];
       v = ld_stream_i32(p.csr + wbeg[a] + (long long)(e - web[a]));
-      const unsigned long long m = ld_cg_u64(Fc + u) & ~ld_cg_u64(p.vis + v);
-      if (m) {
-        const unsigned long long gained = m & ~atomicOr(p.vis + v, m);
-        if (gained) {
-          const long long b0 = ld_nc_i64(p.beg + v);
-          deg = ld_nc_i64(p.beg + v + 1) - b0;
-          // a vertex without edges is never expanded: it gets levels, no frontier bits
-          const unsigned long long prev = deg > 0 ? atomicOr(Fn + v, gained) : ~0ull;
-          act |= gained;
-          for (unsigned long long bits = gained; bits; bits &= bits - 1) {
-            const int sl = __ffsll((long long)bits) - 1;
-            int* o = p.out[sl];
-            if (o) o[v] = (int)(t + 1 - p.join[sl]);
-            if (deg) atomicAdd(&s_msum[sl], (unsigned long long)deg);
-          }
-          first = prev == 0 && deg > 0;
-        }
-      }
+      first = sv_claim(p, t, Fc, Fn, wu[a], v, deg, b0, act, s_msum);
     }
-    // warp-aggregated append of the first claimants to queue t+1
-    const unsigned mask = __ballot_sync(0xffffffffu, first);
-    if (mask) {
-      const long long d = first ? deg : 0;
-      const long long inc = warp_inclusive_scan(d);
-      unsigned long long old = 0;
-      if (lane == 31) old = atomicAdd(&p.ctl->q[qn], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
-      old = __shfl_sync(0xffffffffu, old, 31);
-      if (first) {
-        const unsigned slot = (unsigned)(old & kCountMask) + __popc(mask & ((1u << lane) - 1));
-        p.qids[qn][slot] = v;
-        p.qeb[qn][slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - d));
-      }
-    }
+    sv_enqueue(p, qn, first, v, deg, b0);
     if (threadIdx.x == 0 && rhi < hi) {
       int a = 0, c = kBlock + 1;
       while (c - a > 1) {
@@ -179,6 +223,7 @@ __device__ void sv_tick(const Params& p, long long t, unsigned nparts, unsigned 
     }
     __syncthreads();
     s = (unsigned)next_s;
+  }
   }
   act = __reduce_or_sync(0xffffffffu, (unsigned)act) |
         ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(act >> 32)) << 32);
@@ -202,7 +247,7 @@ __device__ void sv_tick_bu(const Params& p, long long t, unsigned long long runn
   for (long long base = v0; base < v1; base += blockDim.x) {
     const long long v = base + threadIdx.x;
     bool have = false;
-    long long deg = 0;
+    long long deg = 0, vb0 = 0;
     if (v < v1) {
       const unsigned long long vv = ld_cg_u64(p.vis + v);
       const unsigned long long needed = running & ~vv;
@@ -212,6 +257,7 @@ __device__ void sv_tick_bu(const Params& p, long long t, unsigned long long runn
         for (long long e = b0; e < b1 && got != needed; ++e) got |= ld_cg_u64(Fc + ld_stream_i32(p.csr + e)) & needed;
         if (got) {
           deg = b1 - b0;
+          vb0 = b0;
           p.vis[v] = vv | got;
           Fn[v] = got;
           act |= got;
@@ -225,19 +271,7 @@ __device__ void sv_tick_bu(const Params& p, long long t, unsigned long long runn
         }
       }
     }
-    const unsigned mask = __ballot_sync(0xffffffffu, have);
-    if (mask) {
-      const long long d = have ? deg : 0;
-      const long long inc = warp_inclusive_scan(d);
-      unsigned long long old = 0;
-      if (lane == 31) old = atomicAdd(&p.ctl->q[qn], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
-      old = __shfl_sync(0xffffffffu, old, 31);
-      if (have) {
-        const unsigned slot = (unsigned)(old & kCountMask) + __popc(mask & ((1u << lane) - 1));
-        p.qids[qn][slot] = (int)v;
-        p.qeb[qn][slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - d));
-      }
-    }
+    sv_enqueue(p, qn, have, (int)v, deg, vb0);
   }
   act = __reduce_or_sync(0xffffffffu, (unsigned)act) |
         ((unsigned long long)__reduce_or_sync(0xffffffffu, (unsigned)(act >> 32)) << 32);
@@ -309,6 +343,7 @@ __global__ void k_sv_seed(Params p, long long t, int s, int src) {
     const unsigned long long old = atomicAdd(&p.ctl->q[t % 4], ((unsigned long long)d << 31) | 1ull);
     p.qids[t % 4][old & kCountMask] = src;
     p.qeb[t % 4][old & kCountMask] = (unsigned)(old >> 31);
+    p.qbg[t % 4][old & kCountMask] = b0;
   }
 }
 
@@ -337,7 +372,7 @@ struct ServeRequest {
 struct SlotBatch {
   Graph* g = nullptr;
   cudaStream_t stream = nullptr;
-  DevBuf vis, F[3], q[4], qe[4], ctl, out_tab, join_tab;
+  DevBuf vis, F[3], q[4], qe[4], qb[4], ctl, out_tab, join_tab;
   sv::Params p;
   long long tick = 0;
   int req_of_slot[sv::kSlots];
@@ -381,7 +416,9 @@ static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
     if ((st = b.F[i].ensure(V * 8))) return st;
   // a tick queues each vertex at most once, plus the seeds of one round
   for (int i = 0; i < 4; ++i)
-    if ((st = b.q[i].ensure((V + sv::kSlots + 1) * 4)) || (st = b.qe[i].ensure((V + sv::kSlots + 1) * 4))) return st;
+    if ((st = b.q[i].ensure((V + sv::kSlots + 1) * 4)) || (st = b.qe[i].ensure((V + sv::kSlots + 1) * 4)) ||
+        (st = b.qb[i].ensure((V + sv::kSlots + 1) * 8)))
+      return st;
   XBFS_CUDA_TRY(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
   XBFS_CUDA_TRY(cudaMemsetAsync(b.vis.p, 0, V * 8, b.stream));
   for (int i = 0; i < 3; ++i) XBFS_CUDA_TRY(cudaMemsetAsync(b.F[i].p, 0, V * 8, b.stream));
@@ -399,6 +436,7 @@ static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
   for (int i = 0; i < 4; ++i) {
     p.qids[i] = b.q[i].as<int>();
     p.qeb[i] = b.qe[i].as<unsigned>();
+    p.qbg[i] = b.qb[i].as<long long>();
   }
   p.out = b.out_tab.as<int* const>();
   p.join = b.join_tab.as<long long>();
