@@ -109,3 +109,21 @@ def test_directed_graph_and_isolated_sources():
     res = srv.run(gid, src, np.zeros(len(gid)), to_host=True)
     for i, (g, s) in enumerate(zip(gid, src)):
         assert np.array_equal(res["levels"][i], oracle.bfs_queue(cpu[g][0], cpu[g][1], int(s))), i
+
+
+def test_staggered_joins_on_one_power_law_graph():
+    """Requests on one R-MAT graph arriving a few microseconds apart join the
+    batch at different ticks, so ticks where some slots have large frontiers
+    (advanced bottom-up) and others small ones (advanced top-down in the same
+    tick) are the common case; every answer equals the oracle's."""
+    beg, csr = gen_rmat_host(15, 16, 9)
+    g = Graph.from_csr(beg, csr)
+    srcs = pick_sources(beg, 96, 11).astype(np.int32)
+    arr = np.arange(len(srcs), dtype=np.float64) * 15.0
+    srv = Server([g])
+    res = srv.run(np.zeros(len(srcs), dtype=np.int32), srcs, arr, to_host=True)
+    assert len(set(res["admit_us"].tolist())) > 1
+    for i, s in enumerate(srcs):
+        ref = oracle.bfs_queue(beg, csr, int(s))
+        assert np.array_equal(res["levels"][i], ref), f"request {i} (source {s}) differs"
+        assert res["edges_mc"][i] == oracle.edges_mc(beg, ref)

@@ -15,8 +15,12 @@
 //  * Ticks are top-down: the frontier queue (vertex ids with exclusive edge
 //    offsets) is expanded edge-balanced across the GPU; each edge claims the
 //    slots its target lacks with one 64-bit atomicOr, and the first claimant
-//    of a vertex in a tick queues it for the next. A round of ticks runs in
-//    one cooperative launch with one grid barrier per tick. Graphs run
+//    of a vertex in a tick queues it for the next. On symmetric graphs a
+//    slot whose own frontier holds more than E/8 edges advances bottom-up
+//    instead (unvisited vertices probe their neighbours' masks); the other
+//    slots of that tick stay top-down, so a request that joined late never
+//    makes the bottom-up scan read whole adjacency lists. A round of ticks
+//    runs in one cooperative launch with one grid barrier per tick. Graphs run
 //    on their own streams so their ticks overlap on the device; the host
 //    intervenes every K ticks (K grows with a graph's observed depth, so
 //    long-diameter graphs are not host-bound).
@@ -47,6 +51,7 @@ struct Ctl {
   unsigned long long q[4];            // packed (edges << 31) | count, frontier queue ring
   unsigned long long active[kRing];   // OR of the bits gained at each tick of the window
   unsigned long long msum[kSlots];    // per slot: sum of degrees of reached vertices
+  unsigned long long fe[4][kSlots];   // per slot: edges of its frontier, ring by tick like q
 };
 
 struct Params {
@@ -64,12 +69,13 @@ struct Params {
   Ctl* ctl;
 };
 
-// Claim step of one edge (u, v) at tick t (see sv_tick); returns whether
-// this thread queues v for tick t+1, with v's degree and CSR offset.
-__device__ __forceinline__ bool sv_claim(const Params& p, long long t, const unsigned long long* Fc,
-                                         unsigned long long* Fn, int u, int v, long long& deg, long long& b0,
-                                         unsigned long long& act, unsigned long long* s_msum) {
-  const unsigned long long m = ld_cg_u64(Fc + u) & ~ld_cg_u64(p.vis + v);
+// Claim step of one edge (u, v) at tick t (see sv_tick), u offering the
+// slot mask fu; returns whether this thread queues v for tick t+1, with v's
+// degree and CSR offset.
+__device__ __forceinline__ bool sv_claim_m(const Params& p, long long t, unsigned long long fu,
+                                           unsigned long long* Fn, int v, long long& deg, long long& b0,
+                                           unsigned long long& act, unsigned long long* s_msum) {
+  const unsigned long long m = fu & ~ld_cg_u64(p.vis + v);
   if (!m) return false;
   const unsigned long long gained = m & ~atomicOr(p.vis + v, m);
   if (!gained) return false;
@@ -85,6 +91,13 @@ __device__ __forceinline__ bool sv_claim(const Params& p, long long t, const uns
     if (deg) atomicAdd(&s_msum[sl], (unsigned long long)deg);
   }
   return prev == 0 && deg > 0;
+}
+
+// The same with u's whole frontier mask.
+__device__ __forceinline__ bool sv_claim(const Params& p, long long t, const unsigned long long* Fc,
+                                         unsigned long long* Fn, int u, int v, long long& deg, long long& b0,
+                                         unsigned long long& act, unsigned long long* s_msum) {
+  return sv_claim_m(p, t, ld_cg_u64(Fc + u), Fn, v, deg, b0, act, s_msum);
 }
 
 // Warp-aggregated append of the lanes with `have` to queue qn (full warp).
@@ -230,27 +243,96 @@ __device__ void sv_tick(const Params& p, long long t, unsigned nparts, unsigned 
   if (lane == 0 && act) atomicOr(s_act, act);
 }
 
-// Bottom-up tick t, for large frontiers: every vertex still lacking some of
-// the running slots probes its neighbours' frontier masks until it has found
-// all of them or runs out of neighbours. Each vertex is handled by exactly one
-// thread, so visited, next-frontier mask and queue entry are plain writes.
-// Blocks take contiguous vertex ranges.
-__device__ void sv_tick_bu(const Params& p, long long t, unsigned long long running, unsigned nparts,
-                           unsigned part, unsigned long long* s_msum, unsigned long long* s_act) {
+// Top-down part of a mixed tick t: the queue entries whose frontier mask
+// holds bits of `mask` (the slots not advanced bottom-up at this tick) are
+// compacted per block (each block takes an equal share of the entries) and
+// their edges expanded across the block for those bits only.
+__device__ void sv_tick_td_part(const Params& p, long long t, unsigned long long mask, unsigned nparts,
+                                unsigned part, unsigned long long* s_msum, unsigned long long& act) {
+  __shared__ int cu[kBlock];
+  __shared__ unsigned long long cm[kBlock];
+  __shared__ long long cb[kBlock];
+  __shared__ unsigned long long ce[kBlock];
+  __shared__ unsigned long long s_scan[kBlock / 32 + 1];
+  const int qs = (int)(t % 4), qn = (int)((t + 1) % 4);
+  const unsigned cnt = (unsigned)(ld_cg_u64(&p.ctl->q[qs]) & kCountMask);
+  const unsigned i0 = (unsigned)((unsigned long long)cnt * part / nparts);
+  const unsigned i1 = (unsigned)((unsigned long long)cnt * (part + 1) / nparts);
+  const unsigned long long* Fc = p.F[t % 3];
+  unsigned long long* Fn = p.F[(t + 1) % 3];
+  for (unsigned base = i0; base < i1; base += kBlock) {
+    const unsigned i = base + threadIdx.x;
+    int u = 0;
+    unsigned long long fu = 0, d = 0;
+    long long b0 = 0;
+    if (i < i1) {
+      u = p.qids[qs][i];
+      fu = ld_cg_u64(Fc + u) & mask;
+      if (fu) {
+        b0 = p.qbg[qs][i];
+        d = (unsigned long long)(ld_nc_i64(p.beg + u + 1) - b0);
+      }
+    }
+    // (edges << 16) | entries: one scan gives both positions (d < 2^32)
+    unsigned long long tot = 0;
+    const unsigned long long x =
+        block_exclusive_scan<kBlock, unsigned long long>(fu ? (d << 16) | 1ull : 0ull, s_scan, &tot);
+    if (fu) {
+      const int k = (int)(x & 0xffffull);
+      cu[k] = u;
+      cm[k] = fu;
+      cb[k] = b0;
+      ce[k] = x >> 16;
+    }
+    __syncthreads();
+    const int n = (int)(tot & 0xffffull);
+    const unsigned long long T = tot >> 16;
+    for (unsigned long long e0 = 0; e0 < T; e0 += kBlock) {
+      const unsigned long long e = e0 + threadIdx.x;
+      bool first = false;
+      int v = 0;
+      long long deg = 0, vb0 = 0;
+      if (e < T) {
+        int a = 0, c = n;
+        while (c - a > 1) {
+          const int mid = (a + c) >> 1;
+          if (ce[mid] <= e) a = mid; else c = mid;
+        }
+        v = ld_stream_i32(p.csr + cb[a] + (long long)(e - ce[a]));
+        first = sv_claim_m(p, t, cm[a], Fn, v, deg, vb0, act, s_msum);
+      }
+      sv_enqueue(p, qn, first, v, deg, vb0);
+    }
+    __syncthreads();
+  }
+}
+
+// Bottom-up tick t for the slots in `bu` (those whose own frontier is
+// large): every vertex still lacking some of them probes its neighbours'
+// frontier masks until it has found all of them or runs out of neighbours.
+// The slots in `td` (running, with a frontier, but a small one) advance
+// top-down in the same tick: a slot whose frontier is a handful of vertices
+// would otherwise make every vertex scan its whole neighbour list. The two
+// parts claim disjoint bits, so visited and next-frontier words take atomic
+// ORs and the OR that finds v's next mask empty queues v. Blocks take
+// contiguous vertex ranges.
+__device__ void sv_tick_bu(const Params& p, long long t, unsigned long long bu, unsigned long long td,
+                           unsigned nparts, unsigned part, unsigned long long* s_msum, unsigned long long* s_act) {
   const int lane = threadIdx.x & 31;
   const int qn = (int)((t + 1) % 4);
   const unsigned long long* Fc = p.F[t % 3];
   unsigned long long* Fn = p.F[(t + 1) % 3];
+  unsigned long long act = 0;
+  if (td) sv_tick_td_part(p, t, td, nparts, part, s_msum, act);
   const long long per = (p.V + nparts - 1) / nparts;
   const long long v0 = per * part, v1 = (v0 + per < p.V) ? v0 + per : p.V;
-  unsigned long long act = 0;
   for (long long base = v0; base < v1; base += blockDim.x) {
     const long long v = base + threadIdx.x;
     bool have = false;
     long long deg = 0, vb0 = 0;
     if (v < v1) {
       const unsigned long long vv = ld_cg_u64(p.vis + v);
-      const unsigned long long needed = running & ~vv;
+      const unsigned long long needed = bu & ~vv;
       if (needed) {
         const long long b0 = ld_nc_i64(p.beg + v), b1 = ld_nc_i64(p.beg + v + 1);
         unsigned long long got = 0;
@@ -258,8 +340,8 @@ __device__ void sv_tick_bu(const Params& p, long long t, unsigned long long runn
         if (got) {
           deg = b1 - b0;
           vb0 = b0;
-          p.vis[v] = vv | got;
-          Fn[v] = got;
+          atomicOr(p.vis + v, got);
+          have = atomicOr(Fn + v, got) == 0ull;
           act |= got;
           for (unsigned long long bits = got; bits; bits &= bits - 1) {
             const int sl = __ffsll((long long)bits) - 1;
@@ -267,7 +349,6 @@ __device__ void sv_tick_bu(const Params& p, long long t, unsigned long long runn
             if (o) o[v] = (int)(t + 1 - p.join[sl]);
             atomicAdd(&s_msum[sl], (unsigned long long)deg);
           }
-          have = true;
         }
       }
     }
@@ -290,23 +371,36 @@ __device__ void sv_retire(const Params& p, long long t, unsigned nparts, unsigne
 // One round of k ticks from t0 in one cooperative launch, one grid barrier
 // per tick. During tick t the blocks also retire frontier t-1 (its mask
 // buffer is neither read nor written at tick t) and block 0 resets the
-// queue counter of tick t+2 (last used at tick t-2) and, inside the round,
-// the activity word of tick t+1. Every wait is bounded
-// (XBFS_ERR_DEVICE_TIMEOUT).
-// A tick runs bottom-up when its frontier's edges exceed E / kBuRatio (the
-// frontier queue's packed counter is final after the previous barrier, so
-// every block takes the same decision); `running` = the slots in the batch.
+// queue counter and per-slot frontier edges of tick t+2 (last used at tick
+// t-2) and, inside the round, the activity word of tick t+1. Every wait is
+// bounded (XBFS_ERR_DEVICE_TIMEOUT).
+// A slot advances bottom-up at tick t when its own frontier's edges exceed
+// E / kBuRatio, the others top-down (sv_tick_bu); with no such slot the tick
+// is top-down (sv_tick). The per-slot edge counts are final after the
+// previous barrier, so every block takes the same decision. `running` = the
+// slots in the batch.
 constexpr long long kBuRatio = 8;
 
 __global__ void __launch_bounds__(kBlock) k_sv_round(Params p, long long t0, int k, unsigned long long timeout_ns,
                                                      unsigned long long running) {
   __shared__ unsigned long long s_msum[kSlots];
   __shared__ unsigned long long s_act;
+  __shared__ unsigned s_bu[2], s_live[2];
   const unsigned G = gridDim.x, b = blockIdx.x;
   uint32_t epoch = 0;
   for (int i = 0; i < k; ++i) {
     const long long t = t0 + i;
-    if (threadIdx.x < kSlots) s_msum[threadIdx.x] = 0;
+    if (threadIdx.x < kSlots) {
+      s_msum[threadIdx.x] = 0;
+      const unsigned long long f = ld_cg_u64(&p.ctl->fe[t % 4][threadIdx.x]);
+      const bool big = p.allow_bu && ((running >> threadIdx.x) & 1ull) && (long long)f * kBuRatio > p.E;
+      const unsigned bb = __ballot_sync(0xffffffffu, big), lb = __ballot_sync(0xffffffffu, f != 0);
+      if ((threadIdx.x & 31) == 0) {
+        s_bu[threadIdx.x >> 5] = bb;
+        s_live[threadIdx.x >> 5] = lb;
+      }
+      if (b == 0) p.ctl->fe[(t + 2) % 4][threadIdx.x] = 0ull;
+    }
     if (threadIdx.x == 0) s_act = 0;
     if (b == 0 && threadIdx.x == 0) {
       p.ctl->q[(t + 2) % 4] = 0ull;
@@ -315,13 +409,17 @@ __global__ void __launch_bounds__(kBlock) k_sv_round(Params p, long long t0, int
     }
     __syncthreads();
     if (t > 0) sv_retire(p, t - 1, G, b);
-    const unsigned long long qk = ld_cg_u64(&p.ctl->q[t % 4]);
-    if (p.allow_bu && (long long)(qk >> 31) * kBuRatio > p.E)
-      sv_tick_bu(p, t, running, G, b, s_msum, &s_act);
+    const unsigned long long bu = s_bu[0] | ((unsigned long long)s_bu[1] << 32);
+    const unsigned long long live = s_live[0] | ((unsigned long long)s_live[1] << 32);
+    if (bu)
+      sv_tick_bu(p, t, bu, running & live & ~bu, G, b, s_msum, &s_act);
     else
       sv_tick(p, t, G, b, s_msum, &s_act);
     __syncthreads();
-    if (threadIdx.x < kSlots && s_msum[threadIdx.x]) atomicAdd(&p.ctl->msum[threadIdx.x], s_msum[threadIdx.x]);
+    if (threadIdx.x < kSlots && s_msum[threadIdx.x]) {
+      atomicAdd(&p.ctl->msum[threadIdx.x], s_msum[threadIdx.x]);
+      atomicAdd(&p.ctl->fe[(t + 1) % 4][threadIdx.x], s_msum[threadIdx.x]);
+    }
     if (threadIdx.x == 0 && s_act) atomicOr(&p.ctl->active[t % kRing], s_act);
     if (!grid_sync(&p.ctl->bar, G, epoch, timeout_ns)) return;
   }
@@ -336,6 +434,8 @@ __global__ void k_sv_seed(Params p, long long t, int s, int src) {
   if (p.out[s]) p.out[s][src] = 0;
   const long long b0 = p.beg[src], d = p.beg[src + 1] - b0;
   p.ctl->msum[s] = (unsigned long long)d;
+  // no earlier tick gave slot s anything for tick t; the word was reset at t-2
+  p.ctl->fe[t % 4][s] = (unsigned long long)d;
   if (d == 0) return;  // nothing to expand: the request completes at its first tick
   const unsigned long long prev = p.F[t % 3][src];
   p.F[t % 3][src] = prev | bit;
