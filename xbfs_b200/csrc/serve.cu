@@ -64,8 +64,8 @@ struct Params {
   int* qids[4];
   unsigned* qeb[4];
   long long* qbg[4];   // CSR offset of each queued vertex
-  int* const* out;     // device table: output array of each slot (or null)
-  const long long* join;  // device table: join tick of each slot
+  int** out;           // device table: output array of each slot (or null)
+  long long* join;     // device table: join tick of each slot
   Ctl* ctl;
 };
 
@@ -425,13 +425,17 @@ __global__ void __launch_bounds__(kBlock) k_sv_round(Params p, long long t0, int
   }
 }
 
-// Seed slot s at src for tick t (its visited and frontier bit, level 0, a
-// queue entry).
-__global__ void k_sv_seed(Params p, long long t, int s, int src) {
+// Seed slot s at src for tick t: its output array and join tick go into the
+// slot tables (kernel arguments, so the host never copies from pageable
+// memory onto a stream with a round in flight), then its visited and
+// frontier bit, level 0 and a queue entry.
+__global__ void k_sv_seed(Params p, long long t, int s, int src, int* out) {
   if (threadIdx.x != 0) return;
   const unsigned long long bit = 1ull << s;
+  p.out[s] = out;
+  p.join[s] = t;
   p.vis[src] |= bit;
-  if (p.out[s]) p.out[s][src] = 0;
+  if (out) out[src] = 0;
   const long long b0 = p.beg[src], d = p.beg[src + 1] - b0;
   p.ctl->msum[s] = (unsigned long long)d;
   // no earlier tick gave slot s anything for tick t; the word was reset at t-2
@@ -447,8 +451,9 @@ __global__ void k_sv_seed(Params p, long long t, int s, int src) {
   }
 }
 
-// Clear the visited bits of retired slots.
+// Retire the slots in mask: no output array, visited bits cleared.
 __global__ void k_sv_clear(Params p, unsigned long long mask) {
+  if (blockIdx.x == 0 && threadIdx.x < kSlots && ((mask >> threadIdx.x) & 1ull)) p.out[threadIdx.x] = nullptr;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < p.V; v += (long long)gridDim.x * blockDim.x) {
     const unsigned long long x = p.vis[v];
     if (x & mask) p.vis[v] = x & ~mask;
@@ -538,7 +543,7 @@ static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
     p.qeb[i] = b.qe[i].as<unsigned>();
     p.qbg[i] = b.qb[i].as<long long>();
   }
-  p.out = b.out_tab.as<int* const>();
+  p.out = b.out_tab.as<int*>();
   p.join = b.join_tab.as<long long>();
   p.ctl = b.ctl.as<sv::Ctl>();
   for (int s = 0; s < sv::kSlots; ++s) b.req_of_slot[s] = -1;
@@ -697,6 +702,9 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
       }
       const double tf = now_us(t0);
       int max_depth = 0;
+      // the slots leave the tables (k_sv_clear) before their arrays are freed
+      sv::k_sv_clear<<<b.grid, 256, 0, b.stream>>>(b.p, finished);
+      XBFS_CUDA_TRY(cudaGetLastError());
       for (unsigned long long m = finished; m; m &= m - 1) {
         const int sl = __builtin_ctzll(m);
         ServeRequest& r = srv->reqs[b.req_of_slot[sl]];
@@ -712,13 +720,9 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
           srv->in_use -= (size_t)b.g->V * 4;
           r.out = nullptr;
         }
-        int* null = nullptr;
-        XBFS_CUDA_TRY(cudaMemcpyAsync(b.out_tab.as<int*>() + sl, &null, sizeof(int*), cudaMemcpyHostToDevice, b.stream));
         b.req_of_slot[sl] = -1;
         ++done;
       }
-      sv::k_sv_clear<<<b.grid, 256, 0, b.stream>>>(b.p, finished);
-      XBFS_CUDA_TRY(cudaGetLastError());
       b.busy &= ~finished;
       // host every ~1/8 of the depth seen so far, at least every tick
       b.k_ticks = std::max(1, std::min(sv::kRing, max_depth / 8));
@@ -746,10 +750,10 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
         r.admit_us = now_us(t0);
         r.status = 1;
         XBFS_CUDA_TRY(cudaMemsetAsync(r.out, 0xff, need, b.stream));
-        XBFS_CUDA_TRY(cudaMemcpyAsync(b.out_tab.as<int*>() + sl, &r.out, sizeof(int*), cudaMemcpyHostToDevice, b.stream));
-        XBFS_CUDA_TRY(cudaMemcpyAsync(b.join_tab.as<long long>() + sl, &r.join, 8, cudaMemcpyHostToDevice, b.stream));
-        // the seed goes into tick b.issued's frontier
-        sv::k_sv_seed<<<1, 32, 0, b.stream>>>(b.p, b.issued, sl, r.src);
+        // the seed goes into tick b.issued's frontier and records the slot's
+        // output array and join tick
+        sv::k_sv_seed<<<1, 32, 0, b.stream>>>(b.p, b.issued, sl, r.src, r.out);
+        XBFS_CUDA_TRY(cudaGetLastError());
       }
     }
     // issue the next round of every idle batch with running slots; the
