@@ -806,7 +806,8 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
       if (next < order.size()) {
         const double wait = srv->reqs[order[next]].arrival_us - now_us(t0);
         if (wait > 50) {
-          // idle until the next arrival (short sleeps keep latency honest)
+          // spin until the next arrival: a sleep would add its wake-up delay
+          // to that request's latency
           const auto until = t0 + std::chrono::microseconds((long long)srv->reqs[order[next]].arrival_us);
           while (std::chrono::steady_clock::now() < until) {
           }
