@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=32)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the cpu_baseline sample")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own GPU BFS beside its CPU BFS")
+    ap.add_argument("--reference-gpu-sources", type=int, default=4)
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the timed rows")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the learned / batched / multi-graph / serving comparison sections")
     return ap.parse_args()
@@ -66,7 +70,7 @@ class ClockSampler:
         "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80, "sync_boost": 0x10,
     }
 
-    def __init__(self, device: int, period_s: float = 0.02):
+    def __init__(self, device: int, period_s: float = 0.002):
         self.device, self.period = device, period_s
         self.samples: list[tuple[int, int]] = []
         self.max_mhz = None
@@ -225,6 +229,34 @@ def cpu_sample(beg, csr, srcs, budget_s, kind="serial"):
     return edges / t_total / 1e9, done, t_total, threads
 
 
+def check_parity(g, beg, par_src, par_rows, e2e_par, world):
+    """Level rows the timed region and the e2e leg produced, compared with
+    the OpenMP oracle (and the serial FIFO oracle on the first source) on the
+    same graph. Every rank checks its own rows; counts are summed."""
+    import oracle
+    _, csr = g.download()
+    cache = {}
+
+    def ref(s):
+        if s not in cache:
+            cache[s] = oracle.bfs_do(beg, csr, s)
+        return cache[s]
+    checked = mism = 0
+    for s, row in list(zip(par_src, par_rows if par_rows is not None else [])) + list(e2e_par):
+        checked += 1
+        mism += int(not np.array_equal(row, ref(s)))
+    if par_src:
+        checked += 1
+        mism += int(not np.array_equal(par_rows[0], oracle.bfs_queue(beg, csr, par_src[0])))
+    del csr
+    if world > 1:
+        import torch.distributed as dist
+        checked, mism = allreduce([float(checked), float(mism)], dist.ReduceOp.SUM)
+    return {"checked": int(checked), "mismatches": int(mism),
+            "rows": "levels of the last timed chunk (up to 16 sources) and of the first e2e host rows",
+            "oracle": "OpenMP direction-optimising BFS per source, plus the serial FIFO BFS on the first"}
+
+
 # ---------------------------------------------------------------------------
 def run_ours(args):
     import torch
@@ -286,6 +318,10 @@ def run_ours(args):
     t_wall = time.perf_counter() - t_wall0
     value, tot_edges, max_s = job_rate(edges, ev0.elapsed_time(ev1) * 1e-3, world)
     max_ms = max_s * 1e3
+    # level rows of the last timed chunk, kept for the oracle check below
+    n_par = 0 if args.no_parity else min(16, len(plan[-1]))
+    par_src = [int(x) for x in plan[-1][:n_par]]
+    par_rows = rows[:n_par].cpu().numpy() if n_par else None
     del rows
 
     # ---- one xbfs_bfs call per step with the L2 flushed before each (the
@@ -302,6 +338,7 @@ def run_ours(args):
 
     # ---- end to end through the public API with host buffers
     e2e = None
+    e2e_par = []
     if not args.no_e2e:
         # xbfs_bfs_many: one public call for all e2e steps, each step's int32[V]
         # level array copied to pinned host memory while the next traversal runs
@@ -314,6 +351,7 @@ def run_ours(args):
         r = g.bfs_many(e_src, levels=host_rows, opts=opts)
         barrier(world)
         e_gteps, _, _ = job_rate(r.edges_mc, time.perf_counter() - t0, world)
+        e2e_par = [(int(e_src[i]), host_rows[i].copy()) for i in range(min(4, nstep))] if not args.no_parity else []
         single = host_rows[0]
         t1 = time.perf_counter()
         e1 = 0
@@ -340,6 +378,10 @@ def run_ours(args):
                 "kernel": "k_bfs (persistent cooperative level loop)",
                 "algorithmic_bytes_per_launch": b_alg,
                 "mean_launch_ms": round(mean_k, 5)}
+    if traffic:
+        # what DRAM actually moved per launch (ncu) over the same launch time
+        roofline["dram_gbs_ncu"] = round(traffic / (mean_k * 1e-3) / 1e9, 1)
+        roofline["dram_frac_ncu"] = round(traffic / (mean_k * 1e-3) / 1e9 / peak, 4)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -353,6 +395,10 @@ def run_ours(args):
                                 "sample": f"OpenMP direction-optimising BFS (oracle) from {len(odone)} sources, "
                                           f"{osecs:.1f} s"}
         del csr
+    parity = None
+    if not args.no_parity:
+        parity = check_parity(g, beg, par_src, par_rows, e2e_par, world)
+    del par_rows
     depth = statistics.median(r.depth for r in results)
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GTEPS", "n_gpus": world,
@@ -360,12 +406,10 @@ def run_ours(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded Graph500 R-MAT generated on the device)" if args.workload == "rmat"
         else "synthetic (2D 4-neighbour grid)",
-        "config": {"workload": f"{wname} single-source BFS", "V": V, "E": E, "sources": len(srcs),
-                   "policy": args.policy, "seed": args.seed,
-                   "l2": "inputs larger than L2 (CSR of E int32 entries) in the timed back-to-back steps; "
-                         "the per-call figures flush L2 (256 MB write + 256 MB read, untimed) before each call",
-                   "timed_region": "xbfs_bfs_many over the steps' sources, level rows in HBM",
-                   "parallelism": f"replicas x{world}", "median_depth": depth, "levels_by_strategy": strat},
+        "config": workload_config(args, V, E, len(srcs), world),
+        "timed_region": "xbfs_bfs_many over the steps' sources, level rows in HBM; the per-call figures flush "
+                        "L2 (256 MB write + 256 MB read, untimed) before each call",
+        "median_depth": depth, "levels_by_strategy": strat, "parity": parity,
         "per_call_l2_flushed": {"gteps": round(pc_gteps, 3), "steps": pc_steps,
                                 "ms_per_step": round(sum(step_ms) / pc_steps, 5),
                                 "kernel_ms_mean": round(statistics.mean(kernel_ms), 5)},
@@ -464,6 +508,18 @@ def extra_learned(args, g, srcs, opts, lv, stream, flush, flush_rd, plain_gteps)
     return out
 
 
+def batched_roofline(V, E, n, ms):
+    """Batched algorithmic bytes: one pass over the CSR pair per group of 64
+    sources plus the n int32[V] level rows, over the device time."""
+    groups = (n + 63) // 64
+    b_alg = groups * (8 * (V + 1) + 4 * E) + 4 * V * n
+    peak, peak_kind = peak_hbm()
+    ach = b_alg / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+            "peak_source": peak_kind, "algorithmic_bytes_per_call": b_alg,
+            "kernel": "ms::k_msbfs + ms::k_ms_transpose (device time of the call)"}
+
+
 def extra_batched_same_graph(args, g, beg, plain_gteps, wname):
     """512 sources in one batched pass (8 uint64 words per vertex) on the
     bench's own graph, against the plain form's timed value on it."""
@@ -480,7 +536,7 @@ def extra_batched_same_graph(args, g, beg, plain_gteps, wname):
     torch.cuda.empty_cache()
     gteps = best.edges_mc / (best.device_ms * 1e-3) / 1e9
     return {"workload": f"{wname}, 512 sources", "gteps": round(gteps, 3), "ms": round(best.device_ms, 3),
-            "vs_plain": round(gteps / plain_gteps, 3)}
+            "vs_plain": round(gteps / plain_gteps, 3), "roofline": batched_roofline(g.V, g.E, 512, best.device_ms)}
 
 
 def extra_batched(args, plain_ref):
@@ -508,6 +564,7 @@ def extra_batched(args, plain_ref):
     res = {"workload": "rmat-s22-ef16, 512 sources", "gteps": round(best.edges_mc / (best.device_ms * 1e-3) / 1e9, 3),
            "ms": round(best.device_ms, 3), "single_source_gteps_same_graph": round(single, 3)}
     res["vs_single_source"] = round(res["gteps"] / single, 3)
+    res["roofline"] = batched_roofline(g.V, g.E, 512, best.device_ms)
     del out
     g.free()
     torch.cuda.empty_cache()
@@ -534,7 +591,15 @@ def extra_multigraph(args):
         r = g.bfs(int(s))
         t_one += r.device_ms
         mc1 += r.edges_mc
+    b_alg = sum(8 * (g.V + 1) + 4 * g.E + 4 * g.V for g in graphs)
+    peak, peak_kind = peak_hbm()
+    ach = b_alg / (best.device_ms * 1e-3) / 1e9
     res = {"workload": "256 graphs (128 R-MAT s10-18, 128 ER 1e3-2e5)", "gteps": round(best.edges_mc / (best.device_ms * 1e-3) / 1e9, 3),
+           "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(ach / peak, 4), "peak_source": peak_kind,
+                        "algorithmic_bytes_per_launch": b_alg, "kernel": "mg::k_multi",
+                        "note": "sum over graphs of size(beg) + size(csr) + 4V, over the device time of the "
+                                "replayed launch; the whole arena (about 1.2 GB) partly fits the 126 MB L2"},
            "ms": round(best.device_ms, 3), "tuned": cfg, "one_call_per_graph_ms": round(t_one, 3),
            "speedup_vs_one_call_per_graph": round(t_one / best.device_ms, 2)}
     mg.free()
@@ -588,31 +653,92 @@ def extra_serve(args):
     return res
 
 
+def workload_config(args, V, E, n_sources, world):
+    """The config block both arms print (same keys and values for the same
+    command line): the workload, its sizes and seeds, and how L2 is kept out
+    of the timed steps."""
+    if args.workload == "rmat":
+        wname = f"rmat-s{args.scale}-ef{args.ef}"
+    else:
+        wname = f"grid-{args.grid_w}x{args.grid_h}"
+    return {"workload": f"{wname} single-source BFS", "V": int(V), "E": int(E), "sources": int(n_sources),
+            "policy": args.policy, "seed": args.seed,
+            "l2": "inputs larger than L2 (CSR of E int32 entries) in the timed steps",
+            "parallelism": f"replicas x{world}"}
+
+
+def reference_gpu_leg(beg, csr, srcs, k, alpha=0.1):
+    """The reference's own GPU BFS (BFS_ControlFlow, compiled unmodified from
+    the reference sources into oracle/_ref/xbfs_ref_harness by oracle/Makefile)
+    on the same graph and sources, one harness process per source. The
+    harness refuses (exit 3, nothing launched) the inputs on which the
+    reference has known out-of-bounds accesses. GTEPS from the reference's
+    own TD/BU phase timers and from the wall time of its BFS_ControlFlow
+    call (which includes its per-level host work); levels compared with the
+    OpenMP oracle."""
+    import subprocess
+    import tempfile
+
+    import oracle
+    if not os.path.exists(oracle.REF_HARNESS):
+        return {"unavailable": "oracle/_ref/xbfs_ref_harness not built (it needs the reference sources at build time)"}
+    rows = []
+    with tempfile.TemporaryDirectory() as d:
+        bp, cp = os.path.join(d, "g_beg_pos.bin"), os.path.join(d, "g_csr.bin")
+        np.ascontiguousarray(beg, dtype="<i8").tofile(bp)
+        np.ascontiguousarray(csr, dtype="<i4").tofile(cp)
+        for s in srcs[:k]:
+            out = os.path.join(d, "lv.bin")
+            try:
+                r = subprocess.run([oracle.REF_HARNESS, bp, cp, str(int(s)), out, str(alpha), "256", "256"],
+                                   capture_output=True, text=True, timeout=300)
+            except Exception as e:  # timed out or could not start
+                rows.append({"src": int(s), "error": str(e)[:200]})
+                continue
+            try:
+                info = json.loads(r.stderr.strip().splitlines()[-1])
+            except (ValueError, IndexError):  # no record: e.g. no CUDA device
+                rows.append({"src": int(s), "rc": r.returncode, "error": (r.stderr + r.stdout)[-200:]})
+                continue
+            info["rc"] = r.returncode
+            rec = {"src": int(s), "rc": info["rc"]}
+            if info["rc"] == 0 and "kernel_s" in info:
+                lv = np.fromfile(out, dtype="<i4")
+                rec.update(kernel_s=info["kernel_s"], wall_s=info["wall_s"], depth=info.get("levels"),
+                           edges_mc=oracle.edges_mc(beg, lv),
+                           levels_equal_oracle=bool(np.array_equal(lv, oracle.bfs_do(beg, csr, int(s)))))
+            else:
+                rec["skipped"] = info.get("skipped") or info.get("error") or "no result"
+            rows.append(rec)
+    ok = [r for r in rows if "kernel_s" in r]
+    res = {"impl": "BFS_ControlFlow of the reference, unmodified, 256 x 256, alpha 0.1, padding 1",
+           "sources_tried": len(rows), "sources_timed": len(ok)}
+    if ok:
+        mc = sum(r["edges_mc"] for r in ok)
+        res["gteps_phase_timers"] = round(mc / sum(r["kernel_s"] for r in ok) / 1e9, 3)
+        res["gteps_wall"] = round(mc / sum(r["wall_s"] for r in ok) / 1e9, 4)
+        res["ms_phase_timers_per_source"] = round(sum(r["kernel_s"] for r in ok) / len(ok) * 1e3, 3)
+        res["all_levels_equal_oracle"] = all(r["levels_equal_oracle"] for r in ok)
+    res["per_source"] = rows
+    return res
+
+
 def run_reference(args):
-    """The reference's CPU BFS (sweep, bfs_gpu_update.cu:105-127), all host threads."""
+    """The reference's CPU BFS (sweep, bfs_gpu_update.cu:105-127), all host
+    threads, on the same graph and sources as the other arm. The graph and
+    sources come from the oracle's own generator (oracle/gen.c), so this arm
+    loads no product library; the reference's GPU BFS is timed beside it."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import oracle
-    from xbfs_b200 import gen_grid_host, gen_rmat_host, pick_sources
     threads = len(os.sched_getaffinity(0))
-    try:
-        import torch
-        have_gpu = torch.cuda.is_available()
-    except Exception:
-        have_gpu = False
-    if have_gpu:
-        g, wname = make_graph(args, 0)   # input preparation only; not timed
-        beg, csr = g.download()
-        g.free()
-    elif args.workload == "rmat":
-        beg, csr = gen_rmat_host(args.scale, args.ef, args.seed)
-        wname = f"rmat-s{args.scale}-ef{args.ef}"
+    if args.workload == "rmat":
+        beg, csr = oracle.gen_rmat(args.scale, args.ef, args.seed)
     else:
-        beg, csr = gen_grid_host(args.grid_w, args.grid_h)
-        wname = f"grid-{args.grid_w}x{args.grid_h}"
-    srcs = pick_sources(beg, args.sources, args.seed)
+        beg, csr = oracle.gen_grid(args.grid_w, args.grid_h)
+    srcs = oracle.pick_sources(beg, args.sources, args.seed)
     for i in range(args.warmup):
         oracle.bfs_sweep(beg, csr, srcs[i % len(srcs)], threads)
     t_total, edges = 0.0, 0
@@ -633,14 +759,17 @@ def run_reference(args):
         "metric": METRIC, "value": round(value, 4), "unit": "GTEPS", "n_gpus": world, "steps": done,
         "warmup": args.warmup, "ms_per_step": round(t_total / done * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "impl": "reference",
-        "data": "synthetic (seeded Graph500 R-MAT)",
-        "config": {"workload": f"{wname} single-source BFS", "V": len(beg) - 1, "E": int(beg[-1]),
-                   "sources": len(srcs), "seed": args.seed},
+        "data": "synthetic (seeded Graph500 R-MAT)" if args.workload == "rmat" else "synthetic (2D 4-neighbour grid)",
+        "config": workload_config(args, len(beg) - 1, int(beg[-1]), len(srcs), world),
+        "timed_region": f"the reference's CPU sweep BFS (bfs_gpu_update.cu:105-127) restated, one source per step, "
+                        f"{threads} threads",
         "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": threads, "kind": "port",
                          "sample": f"reference sweep BFS (bfs_gpu_update.cu:105-127) restated, {done} sources, "
                                    f"{threads} threads"},
         "e2e": {"value": round(value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_reference_gpu:
+        out["reference_gpu"] = reference_gpu_leg(beg, csr, srcs, args.reference_gpu_sources)
     print(json.dumps(out), flush=True)
 
 

@@ -188,14 +188,19 @@ xbfs_status xbfs_bfs_many(xbfs_graph* g, const int32_t* srcs, int32_t n, int32_t
  * results as xbfs_bfs, but the traversal workspace comes from one fixed
  * static device array of XBFS_NOALLOC_SCRATCH_BYTES per device, not from
  * cudaMalloc. Requirements and limits:
- *  - levels (and parents, if not NULL) must be device memory on g's device;
+ *  - levels (and parents, if not NULL) must be device memory on g's device
+ *    (XBFS_ERR_INVALID_ARG otherwise, host memory and other devices' memory
+ *    included);
  *  - graphs whose workspace exceeds the array are refused with
  *    XBFS_ERR_UNSUPPORTED and a message giving the bytes needed (R-MAT with
  *    edge factor 16 fits up to about 2^20 vertices; xbfs_bfs has no limit);
- *  - the first call on a device resolves the array's address
- *    (cudaGetSymbolAddress, which also makes the runtime load the module
- *    holding the array) and sets the kernel's launch attributes; make that
- *    first call before any stream capture begins;
+ *  - every call resolves the array's address in the current context
+ *    (cudaGetSymbolAddress; the first one also makes the runtime load the
+ *    module holding the array); the first call on a device also sets the
+ *    kernel's launch attributes: make that first call before any stream
+ *    capture begins;
+ *  - wait_timeout_us and test_absent_block bound and test the device-side
+ *    waits exactly as in xbfs_bfs;
  *  - nothing in the array has to start at zero: each call clears the
  *    visited/frontier bitmaps and the control block it reads first;
  *  - calls on the same device share the one array: calls that overlap in time

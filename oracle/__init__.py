@@ -12,6 +12,11 @@ What is here (oracle.c):
   reference_schedule  the reference's per-level direction switch
              (bfs_adaptiveFQ_wb_async.cuh:946-1078, 1114) replayed from levels
 
+Input preparation of the oracle side (gen.c): gen_rmat, gen_grid and
+pick_sources build the same seeded graphs and sources as the library's
+generators with code of their own, so bench.py's reference arm needs no
+product library and the tests can compare the two builds.
+
 Parity pins: tests/golden/ holds level arrays produced by the reference's own
 GPU path (oracle/_ref/xbfs_ref_harness, built from the reference sources by
 oracle/Makefile and run on a B200; script: tests/golden/make_golden.py).
@@ -31,8 +36,8 @@ REF_HARNESS = os.path.join(REF_DIR, "xbfs_ref_harness")
 
 
 def build() -> str:
-    if (not os.path.exists(_LIB) or
-            os.path.getmtime(_LIB) < os.path.getmtime(os.path.join(_HERE, "oracle.c"))):
+    srcs = [os.path.join(_HERE, f) for f in ("oracle.c", "gen.c")]
+    if not os.path.exists(_LIB) or any(os.path.getmtime(_LIB) < os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
     return _LIB
 
@@ -51,6 +56,16 @@ def _load():
     lib.oracle_check_tree.argtypes = [p, p, C.c_int64, C.c_int32, p, p]
     lib.oracle_edges_mc.restype = C.c_int64
     lib.oracle_edges_mc.argtypes = [p, C.c_int64, p]
+    pp = C.POINTER(C.c_void_p)
+    lib.oracle_gen_rmat.restype = C.c_int32
+    lib.oracle_gen_rmat.argtypes = [C.c_int32, C.c_int32, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                                    pp, pp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.oracle_gen_grid.restype = C.c_int32
+    lib.oracle_gen_grid.argtypes = [C.c_int32, C.c_int32, pp, pp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.oracle_pick_sources.restype = C.c_int32
+    lib.oracle_pick_sources.argtypes = [p, C.c_int64, C.c_int32, C.c_uint64, p]
+    lib.oracle_free.restype = None
+    lib.oracle_free.argtypes = [C.c_void_p]
     return lib
 
 
@@ -150,3 +165,39 @@ def reference_schedule(beg, levels, alpha: float = 0.1) -> list[int]:
         tags.append(tag)
         tag_prev = tag
     return tags
+
+
+def _take(pb, pc, V, E) -> tuple[np.ndarray, np.ndarray]:
+    beg = np.ctypeslib.as_array(C.cast(pb, C.POINTER(C.c_int64)), shape=(V.value + 1,)).copy()
+    csr = np.ctypeslib.as_array(C.cast(pc, C.POINTER(C.c_int32)), shape=(max(E.value, 1),))[: E.value].copy()
+    _lib.oracle_free(pb)
+    _lib.oracle_free(pc)
+    return beg, csr
+
+
+def gen_rmat(scale: int, edge_factor: int, seed: int = 1, a: float = 0.57, b: float = 0.19,
+             c: float = 0.19) -> tuple[np.ndarray, np.ndarray]:
+    """Seeded Graph500 R-MAT CSR (symmetric, deduplicated, no self-loops)."""
+    pb, pc, V, E = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int64()
+    rc = _lib.oracle_gen_rmat(scale, edge_factor, seed, a, b, c, C.byref(pb), C.byref(pc), C.byref(V), C.byref(E))
+    if rc != 0:
+        raise MemoryError(f"oracle_gen_rmat failed ({rc})") if rc == -2 else ValueError("bad R-MAT arguments")
+    return _take(pb, pc, V, E)
+
+
+def gen_grid(width: int, height: int) -> tuple[np.ndarray, np.ndarray]:
+    """2D 4-neighbour grid CSR, vertex r * width + c."""
+    pb, pc, V, E = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int64()
+    rc = _lib.oracle_gen_grid(width, height, C.byref(pb), C.byref(pc), C.byref(V), C.byref(E))
+    if rc != 0:
+        raise MemoryError(f"oracle_gen_grid failed ({rc})") if rc == -2 else ValueError("bad grid arguments")
+    return _take(pb, pc, V, E)
+
+
+def pick_sources(beg, k: int, seed: int = 1) -> np.ndarray:
+    """k seeded sources, uniform over vertices with degree > 0."""
+    beg = np.ascontiguousarray(beg, dtype=np.int64)
+    out = np.empty(max(k, 1), dtype=np.int32)
+    if _lib.oracle_pick_sources(beg.ctypes.data, len(beg) - 1, k, seed, out.ctypes.data) != 0:
+        raise ValueError("graph has no edges")
+    return out[:k]

@@ -77,3 +77,21 @@ def test_reference_arm_under_torchrun_prints_once():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] in ("port", "reference") and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["config"]["workload"] == "rmat-s12-ef8 single-source BFS" and d["config"]["sources"] == 4
+    assert set(d["config"]) == {"workload", "V", "E", "sources", "policy", "seed", "l2", "parallelism"}
+    assert "reference_gpu" in d
+
+
+def test_reference_arm_loads_no_product_library():
+    """The reference arm builds its graph and sources with the oracle's own
+    generator: libxbfs.so must not be mapped into its process."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--scale', '12', '--ef', '8', "
+            "'--steps', '2', '--warmup', '1', '--sources', '4', '--no-reference-gpu']; "
+            "runpy.run_path('bench.py', run_name='__main__'); "
+            "print('MAPPED', any('libxbfs' in l for l in open('/proc/self/maps')))")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=ROOT,
+                       env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "MAPPED False" in r.stdout
+    d = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][0])
+    assert d["config"]["E"] > 0 and d["config"]["policy"] == "heuristic" and "reference_gpu" not in d

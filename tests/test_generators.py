@@ -67,3 +67,24 @@ def test_file_roundtrip(tmp_path):
     assert os.path.getsize(tmp_path / "g_csr.bin") == 4 * len(c)
     b2, c2 = read_csr(str(tmp_path / "g_beg_pos.bin"), str(tmp_path / "g_csr.bin"))
     assert np.array_equal(b, b2) and np.array_equal(c, c2)
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(6, 4, 1), (10, 16, 2), (13, 32, 3), (16, 16, 4), (18, 8, 5)])
+def test_oracle_side_generator_builds_the_same_rmat(scale, ef, seed):
+    """The reference arm of bench.py builds its graph and sources with the
+    oracle's own generator (oracle/gen.c: per-vertex buckets, not the
+    library's key sort); both builds must give the same CSR and sources."""
+    import oracle
+    b1, c1 = oracle.gen_rmat(scale, ef, seed)
+    b2, c2 = gen_rmat_host(scale, ef, seed)
+    assert np.array_equal(b1, b2) and np.array_equal(c1, c2)
+    check_csr_contract(b1, c1)
+    assert np.array_equal(oracle.pick_sources(b1, 64, seed), pick_sources(b2, 64, seed))
+
+
+def test_oracle_side_generator_builds_the_same_grid():
+    import oracle
+    for W, H in [(1, 1), (1, 7), (5, 1), (4, 3), (300, 200)]:
+        b1, c1 = oracle.gen_grid(W, H)
+        b2, c2 = gen_grid_host(W, H)
+        assert np.array_equal(b1, b2) and np.array_equal(c1, c2)

@@ -61,16 +61,64 @@ def test_two_calls_in_a_row_match_xbfs_bfs(kind):
 
 def test_policies_and_levels_only():
     import torch
+    from xbfs_b200 import learned
     beg, csr = gen_rmat_host(14, 16, 5)
     g = Graph.from_csr(beg, csr)
     s = int(pick_sources(beg, 1, 9)[0])
     ref = oracle.bfs_queue(beg, csr, s)
     lv = torch.empty(g.V, dtype=torch.int32, device="cuda:0")
-    for opts in (BfsOptions(policy="heuristic"), BfsOptions(policy="beamer"), BfsOptions(async_bu=False),
-                 BfsOptions(policy="forced", forced=["td_queue", "td_scan", "bu", "bu", "td_scan"])):
-        noalloc(g, s, lv, None, opts)
-        assert np.array_equal(lv.cpu().numpy(), ref)
-        assert np.array_equal(g.bfs(s, opts=opts).levels, ref)
+    w, _ = learned.load(learned.DEFAULT_WEIGHTS)
+    learned.install(w, device=0)   # the learned switch stages its weights in shared memory
+    try:
+        for opts in (BfsOptions(policy="heuristic"), BfsOptions(policy="beamer"), BfsOptions(async_bu=False),
+                     BfsOptions(policy="forced", forced=["td_queue", "td_scan", "bu", "bu", "td_scan"]),
+                     BfsOptions(policy="mlp")):
+            noalloc(g, s, lv, None, opts)
+            assert np.array_equal(lv.cpu().numpy(), ref)
+            assert np.array_equal(g.bfs(s, opts=opts).levels, ref)
+    finally:
+        learned.install(None, device=0)
+    g.free()
+
+
+def test_callers_stream():
+    """opts.stream: the traversal runs on the caller's stream."""
+    import torch
+    beg, csr = gen_rmat_host(13, 16, 8)
+    g = Graph.from_csr(beg, csr)
+    st = torch.cuda.Stream()
+    lv = torch.empty(g.V, dtype=torch.int32, device="cuda:0")
+    for s in pick_sources(beg, 2, 3):
+        with torch.cuda.stream(st):
+            noalloc(g, int(s), lv, None, BfsOptions(stream=st.cuda_stream))
+        st.synchronize()
+        assert np.array_equal(lv.cpu().numpy(), oracle.bfs_queue(beg, csr, int(s)))
+    g.free()
+
+
+def test_bounded_wait_and_the_next_call():
+    """wait_timeout_us bounds the device-side waits as in xbfs_bfs: one CTA
+    leaves before its first grid barrier (test_absent_block), the others give
+    up after 20 ms, the call returns XBFS_ERR_DEVICE_TIMEOUT, and the next
+    call on the same array is correct (it clears what it reads first)."""
+    import time
+
+    import torch
+    from xbfs_b200._lib import XBFS_ERR_DEVICE_TIMEOUT
+    beg, csr = gen_rmat_host(14, 16, 3)
+    g = Graph.from_csr(beg, csr)
+    s = int(pick_sources(beg, 1, 2)[0])
+    lv = torch.empty(g.V, dtype=torch.int32, device="cuda:0")
+    t0 = time.perf_counter()
+    with pytest.raises(XbfsError) as e:
+        noalloc(g, s, lv, None, BfsOptions(wait_timeout_us=20000, test_absent_block=3))
+    assert e.value.status == XBFS_ERR_DEVICE_TIMEOUT
+    assert time.perf_counter() - t0 < 5.0   # the 20 ms bound, not the 10 s default
+    pa = torch.empty(g.V, dtype=torch.int32, device="cuda:0")
+    noalloc(g, s, lv, pa)
+    levels = lv.cpu().numpy()
+    assert np.array_equal(levels, oracle.bfs_queue(beg, csr, s))
+    assert oracle.check_tree(beg, csr, s, levels, pa.cpu().numpy()) == 0
     g.free()
 
 

@@ -1919,43 +1919,71 @@ extern cudaError_t noalloc_scratch_address(void** ptr);
 
 namespace {
 
+// Shared memory of a traversal launch: the learned switch's weight copy at
+// the end of Smem is only allocated for launches that use it (the rest of
+// the SM's unified storage stays L1).
+constexpr size_t kSmemNoMlp = sizeof(Smem) - sizeof(((Smem*)0)->mlp_w);
+
 struct NoallocDevice {
   bool ready = false;
-  unsigned char* scratch = nullptr;
-  int grid[2] = {0, 0};  // resident CTAs of k_bfs<false>, k_bfs<true>
+  int grid[2][2] = {{0, 0}, {0, 0}};  // resident CTAs: [parents on][learned switch on]
 };
 std::mutex g_noalloc_mu;
 NoallocDevice g_noalloc[64];
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Per-device set-up, run once with `device` current: the scratch address and
-// the launch shape of both kernel instantiations.
+// Per-device set-up, run once with `device` current: the launch shapes of
+// both kernel instantiations, with and without the learned switch's shared
+// memory. The scratch address itself is resolved again on every call
+// (noalloc_scratch), so a context that was reset and re-created gets the
+// address of the array in its own module image.
 xbfs_status noalloc_setup(int device, NoallocDevice** out) {
   if (device < 0 || device >= 64) return set_error(XBFS_ERR_INVALID_ARG, "device %d out of range", device);
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   NoallocDevice& d = g_noalloc[device];
   if (!d.ready) {
-    void* ptr = nullptr;
-    const cudaError_t e = noalloc_scratch_address(&ptr);
-    if (e != cudaSuccess || !ptr)
-      return set_error(XBFS_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed on device %d: %s",
-                       device, cudaGetErrorString(e));
     int nsm = 0;
     XBFS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     const void* fns[2] = {(const void*)k_bfs<false>, (const void*)k_bfs<true>};
     for (int i = 0; i < 2; ++i) {
       XBFS_CUDA_TRY(cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)));
-      int per_sm = 0;
-      XBFS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fns[i], kBlock, sizeof(Smem)));
-      if (per_sm < 1) return set_error(XBFS_ERR_INTERNAL, "traversal kernel cannot be resident");
-      d.grid[i] = nsm * per_sm;
+      for (int m = 0; m < 2; ++m) {
+        int per_sm = 0;
+        XBFS_CUDA_TRY(
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fns[i], kBlock, m ? sizeof(Smem) : kSmemNoMlp));
+        if (per_sm < 1) return set_error(XBFS_ERR_INTERNAL, "traversal kernel cannot be resident");
+        d.grid[i][m] = nsm * per_sm;
+      }
     }
-    d.scratch = (unsigned char*)ptr;
     d.ready = true;
   }
   *out = &d;
   return XBFS_OK;
+}
+
+// Device address of the static scratch in the current context; checked.
+xbfs_status noalloc_scratch(int device, unsigned char** out) {
+  void* ptr = nullptr;
+  const cudaError_t e = noalloc_scratch_address(&ptr);
+  if (e != cudaSuccess || !ptr) {
+    cudaGetLastError();
+    return set_error(XBFS_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed on device %d: %s", device,
+                     cudaGetErrorString(e));
+  }
+  *out = (unsigned char*)ptr;
+  return XBFS_OK;
+}
+
+// Device memory of `device` (plain or managed): the traversal kernel writes
+// the outputs directly.
+bool on_device(const void* ptr, int device) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == device;
 }
 
 }  // namespace
@@ -1987,13 +2015,17 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
   if (!(o.alpha > 0)) o.alpha = 0.1f;
 
   DeviceGuard dg(g->device);
-  if (!is_device_pointer(levels))
-    return set_error(XBFS_ERR_INVALID_ARG, "xbfs_bfs_noalloc needs levels in device memory");
-  if (parents && !is_device_pointer(parents))
-    return set_error(XBFS_ERR_INVALID_ARG, "xbfs_bfs_noalloc needs parents in device memory");
+  if (!on_device(levels, g->device))
+    return set_error(XBFS_ERR_INVALID_ARG, "xbfs_bfs_noalloc needs levels in device memory of the graph's device %d",
+                     g->device);
+  if (parents && !on_device(parents, g->device))
+    return set_error(XBFS_ERR_INVALID_ARG, "xbfs_bfs_noalloc needs parents in device memory of the graph's device %d",
+                     g->device);
   NoallocDevice* dev = nullptr;
   xbfs_status st = noalloc_setup(g->device, &dev);
   if (st) return st;
+  unsigned char* base = nullptr;
+  if ((st = noalloc_scratch(g->device, &base))) return st;
 
   // ---- carve the scratch; refuse graphs whose workspace does not fit
   const size_t nw = (size_t)((g->V + 31) / 32 + 64);
@@ -2032,7 +2064,6 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
                      "graph needs %zu bytes of traversal scratch (V = %lld); the static scratch of "
                      "xbfs_bfs_noalloc holds %llu bytes (XBFS_NOALLOC_SCRATCH_BYTES): use xbfs_bfs",
                      off, (long long)g->V, (unsigned long long)XBFS_NOALLOC_SCRATCH_BYTES);
-  unsigned char* base = dev->scratch;
 
   // ---- kernel parameters: as setup_params, with the workspace in the scratch
   Params p;
@@ -2070,7 +2101,9 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
   p.medium_max = o.medium_max;
   p.beamer_alpha = o.beamer_alpha > 0 ? o.beamer_alpha : 14.f;
   p.beamer_beta = o.beamer_beta > 0 ? o.beamer_beta : 24.f;
-  p.timeout_ns = 10ull * 1000 * 1000 * 1000;
+  p.timeout_ns = o.wait_timeout_us > 0 ? (unsigned long long)o.wait_timeout_us * 1000ull
+                                        : 10ull * 1000 * 1000 * 1000;
+  p.absent_block = o.test_absent_block;
   p.max_levels = g->V + 2;
   extern const float* mlp_device_weights(int device);
   p.mlp = mlp_device_weights(g->device);
@@ -2081,8 +2114,10 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
   p.stop_level = LLONG_MAX;
   p.resume = 0;
   const bool par_on = parents != nullptr;
+  const bool mlp_on = p.policy == XBFS_POLICY_MLP;
   const void* kfn = par_on ? (const void*)k_bfs<true> : (const void*)k_bfs<false>;
-  int grid = dev->grid[par_on ? 1 : 0];
+  const size_t smem = mlp_on ? sizeof(Smem) : kSmemNoMlp;
+  int grid = dev->grid[par_on ? 1 : 0][mlp_on ? 1 : 0];
   if (o.grid_dim > 0 && o.grid_dim < grid) grid = o.grid_dim;
 
   // ---- initial state (the same steps as init_state) and the launch
@@ -2097,7 +2132,7 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
   k_seed<<<1, 32, 0, s>>>(p, src, par_on ? 1 : 0);
   XBFS_CUDA_TRY(cudaGetLastError());
   void* args[] = {&p};
-  XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, sizeof(Smem), s));
+  XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, smem, s));
   Ctl hctl;
   XBFS_CUDA_TRY(cudaMemcpyAsync(&hctl, p.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   XBFS_CUDA_TRY(cudaStreamSynchronize(s));
