@@ -91,6 +91,16 @@ int main(int argc, char** argv) {
   const std::string workload = pos[9];
   const int padding = atoi(pos[10].c_str());
   printf("alpha = %g\n", alpha);
+  // refused before any device work: the reference's bottom-up update is only
+  // correct for padding 1 (bfs_adaptiveFQ_wb_async.cuh:739-775)
+  if (padding != 1) {
+    fprintf(stderr, "bfs: padding = %d: only 1 is supported\n", padding);
+    return 2;
+  }
+  if (src < 0) {
+    fprintf(stderr, "bfs: source %d is negative\n", src);
+    return 2;
+  }
 
   xbfs_graph* g = nullptr;
   xbfs_status st = xbfs_graph_load(beg_file, csr_file, gpu, &g);
