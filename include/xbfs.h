@@ -262,6 +262,37 @@ xbfs_status xbfs_serve_create(xbfs_graph* const* graphs, int32_t n, int32_t devi
 xbfs_status xbfs_serve_run(xbfs_server* s, int32_t n, const int32_t* graph, const int32_t* src,
                            const double* arrival_us, int32_t keep_outputs, double* admit_us, double* finish_us,
                            int64_t* edges_mc, int32_t** levels, double* wall_us);
+/* Online mode: the same engine in the server's own host thread, fed as
+ * requests arrive. xbfs_serve_start starts it (the server must not be in a
+ * xbfs_serve_run call; a running server refuses xbfs_serve_run with
+ * XBFS_ERR_BUSY). xbfs_serve_submit queues one request and returns at once
+ * with its ticket; it is admitted when a slot of its graph and room in the
+ * HBM budget are free, joins the running batch at its next level step, and
+ * leaves when complete. output: 0 = only the edge count and times are kept;
+ * 1 = the level array stays on the device (xbfs_serve_poll returns it; free
+ * with xbfs_serve_release); 2 = it is copied into levels_host (V int32,
+ * page-locked memory lets the copy overlap) before the request counts as
+ * done. Kept device arrays count against the budget: requests they block
+ * wait for a release. Any host thread may submit and poll. */
+typedef struct xbfs_serve_result {
+  int32_t struct_size;
+  int32_t state;       /* 0 waiting, 1 running (or copying out), 2 done, 3 dropped at stop */
+  double submit_us;    /* times since xbfs_serve_start */
+  double admit_us;     /* -1 until admitted */
+  double finish_us;    /* -1 until done */
+  int64_t edges_mc;    /* Graph500 m_c of the traversal (when done) */
+  int32_t* levels_dev; /* output 1: the device level array (when done) */
+} xbfs_serve_result;
+xbfs_status xbfs_serve_start(xbfs_server* s);
+xbfs_status xbfs_serve_submit(xbfs_server* s, int32_t graph, int32_t src, int32_t output, int32_t* levels_host,
+                              int64_t* ticket);
+/* State of a request. wait_us: 0 = look only, > 0 = wait up to that long,
+ * < 0 = wait until done. Returns XBFS_OK when done (result filled),
+ * XBFS_ERR_BUSY while waiting or running, or the engine's error. */
+xbfs_status xbfs_serve_poll(xbfs_server* s, int64_t ticket, int64_t wait_us, xbfs_serve_result* out);
+/* Lets every submitted request complete, then stops the thread. Requests
+ * that only kept device arrays block at that point are dropped (state 3). */
+xbfs_status xbfs_serve_stop(xbfs_server* s);
 xbfs_status xbfs_serve_release(xbfs_server* s, int32_t* levels_dev, int64_t V);
 /* Copies a kept level array (V entries) to host memory, then releases it. */
 xbfs_status xbfs_serve_fetch(xbfs_server* s, int32_t* levels_dev, int64_t V, int32_t* host_out);

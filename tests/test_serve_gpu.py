@@ -127,3 +127,64 @@ def test_staggered_joins_on_one_power_law_graph():
         ref = oracle.bfs_queue(beg, csr, int(s))
         assert np.array_equal(res["levels"][i], ref), f"request {i} (source {s}) differs"
         assert res["edges_mc"][i] == oracle.edges_mc(beg, ref)
+
+
+def test_online_submit_while_rounds_run_and_poll():
+    """Online mode: requests submitted from two host threads while earlier
+    ones run (the grid's traversal is hundreds of level steps long), with all
+    three output modes; every answer equals the oracle's, and a trace replay
+    is refused while the server runs online."""
+    import threading
+    import time
+
+    from xbfs_b200._lib import XBFS_ERR_BUSY, XbfsError
+    cpu, graphs = setup(3)
+    cpu.append(gen_grid_host(400, 300))
+    graphs.append(Graph.from_csr(*cpu[-1]))
+    srv = Server(graphs)
+    srv.start()
+    with pytest.raises(XbfsError) as e:
+        srv.run(np.zeros(1, dtype=np.int32), np.zeros(1, dtype=np.int32), np.zeros(1))
+    assert e.value.status == XBFS_ERR_BUSY
+    rng = np.random.default_rng(4)
+    subs, lock = [], threading.Lock()
+
+    def submitter(seed, n):
+        r = np.random.default_rng(seed)
+        for i in range(n):
+            g = int(r.integers(0, len(graphs)))
+            s = int(pick_sources(cpu[g][0], 1, seed * 100 + i)[0])
+            out = ("none", "device", "host")[i % 3]
+            t = srv.submit(g, s, output=out)
+            with lock:
+                subs.append((t, g, s, out))
+            time.sleep(float(r.exponential(2e-4)))
+
+    first = srv.submit(len(graphs) - 1, 0, output="host")   # a long traversal in flight
+    subs.append((first, len(graphs) - 1, 0, "host"))
+    assert srv.poll(first) is None   # still running right after submission
+    ths = [threading.Thread(target=submitter, args=(k + 1, 40)) for k in range(2)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    seen_overlap = False
+    for t, g, s, out in subs:
+        res = srv.poll(t, wait_us=-1)
+        ref = oracle.bfs_queue(cpu[g][0], cpu[g][1], s)
+        assert res["edges_mc"] == oracle.edges_mc(cpu[g][0], ref), (t, g, s)
+        assert res["finish_us"] >= res["admit_us"] >= res["submit_us"] - 1
+        if out == "host":
+            assert np.array_equal(res["levels"], ref), (t, g, s)
+        elif out == "device":
+            assert np.array_equal(srv.fetch(res["levels_dev"], graphs[g].V), ref), (t, g, s)
+        if t != first and res["admit_us"] < srv.poll(first)["finish_us"]:
+            seen_overlap = True   # admitted while the long traversal was running
+    assert seen_overlap
+    srv.stop()
+    # after stop, a trace replay on the same server works again
+    gid, src, arr = trace(cpu[:4], 20, 1e5, 9)
+    res = srv.run(gid, src, arr, to_host=True)
+    for i, (g, s) in enumerate(zip(gid, src)):
+        assert np.array_equal(res["levels"][i], oracle.bfs_queue(cpu[g][0], cpu[g][1], int(s)))
+    srv.free()

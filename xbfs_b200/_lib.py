@@ -100,6 +100,12 @@ def _load() -> C.CDLL:
 
 lib = _load()
 
+
+class ServeResult(C.Structure):
+    _fields_ = [("struct_size", C.c_int32), ("state", C.c_int32), ("submit_us", C.c_double),
+                ("admit_us", C.c_double), ("finish_us", C.c_double), ("edges_mc", C.c_int64),
+                ("levels_dev", C.c_void_p)]
+
 _p = C.c_void_p
 _i32, _i64, _u64, _f32, _f64 = C.c_int32, C.c_int64, C.c_uint64, C.c_float, C.c_double
 _PI64 = C.POINTER(C.c_int64)
@@ -145,6 +151,10 @@ SIGNATURES = {
     "xbfs_level_costs": (_i32, [_p, _i32, _i32, _i32, _p, C.POINTER(LevelTrace), _PI32]),
     "xbfs_serve_create": (_i32, [C.POINTER(_p), _i32, _i32, _i64, C.POINTER(_p)]),
     "xbfs_serve_run": (_i32, [_p, _i32, _p, _p, _p, _i32, _p, _p, _p, _p, C.POINTER(C.c_double)]),
+    "xbfs_serve_start": (_i32, [_p]),
+    "xbfs_serve_submit": (_i32, [_p, _i32, _i32, _i32, _p, _PI64]),
+    "xbfs_serve_poll": (_i32, [_p, _i64, _i64, C.POINTER(ServeResult)]),
+    "xbfs_serve_stop": (_i32, [_p]),
     "xbfs_serve_release": (_i32, [_p, _p, _i64]),
     "xbfs_serve_fetch": (_i32, [_p, _p, _i64, _p]),
     "xbfs_serve_free": (None, [_p]),

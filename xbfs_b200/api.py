@@ -391,6 +391,7 @@ class Server:
         check(lib.xbfs_serve_create(arr, len(graphs), device, int(hbm_budget_bytes), C.byref(h)))
         self._h = h
         self.graphs = list(graphs)
+        self._host = {}
 
     def run(self, graph_ids, srcs, arrival_us, keep_outputs: bool = False, to_host: bool = False) -> dict:
         """Replay a request trace. ``keep_outputs``: return device level arrays
@@ -425,6 +426,48 @@ class Server:
             out["levels"] = host
         return out
 
+    # -- online mode -----------------------------------------------------------
+    OUTPUTS = {"none": 0, "device": 1, "host": 2}
+
+    def start(self) -> None:
+        """Run the engine in the server's own thread; requests come from submit()."""
+        check(lib.xbfs_serve_start(self._h))
+        self._host = {}
+
+    def submit(self, graph: int, src: int, output: str = "none", levels: Optional[np.ndarray] = None) -> int:
+        """Queue one request; returns its ticket at once. ``output``: "none"
+        (edge count and times only), "device" (kept level array, see poll /
+        fetch), "host" (copied into ``levels`` or a new array before done)."""
+        mode = self.OUTPUTS[output]
+        if mode == 2 and levels is None:
+            levels = np.empty(self.graphs[graph].V, dtype=np.int32)
+        t = C.c_int64(0)
+        check(lib.xbfs_serve_submit(self._h, int(graph), int(src), mode,
+                                    levels.ctypes.data if mode == 2 else None, C.byref(t)))
+        if mode == 2:
+            self._host[t.value] = levels
+        return t.value
+
+    def poll(self, ticket: int, wait_us: int = 0) -> Optional[dict]:
+        """The request's result when done (None while it waits or runs);
+        ``wait_us`` < 0 waits until done."""
+        r = _lib.ServeResult()
+        r.struct_size = C.sizeof(_lib.ServeResult)
+        st = lib.xbfs_serve_poll(self._h, int(ticket), int(wait_us), C.byref(r))
+        if st == _lib.XBFS_ERR_BUSY:
+            return None
+        check(st)
+        out = {"submit_us": r.submit_us, "admit_us": r.admit_us, "finish_us": r.finish_us,
+               "latency_us": r.finish_us - r.submit_us, "edges_mc": r.edges_mc}
+        if r.levels_dev:
+            out["levels_dev"] = r.levels_dev
+        if ticket in self._host:
+            out["levels"] = self._host.pop(ticket)
+        return out
+
+    def stop(self) -> None:
+        check(lib.xbfs_serve_stop(self._h))
+
     def fetch(self, ptr: int, V: int) -> np.ndarray:
         """Copy one kept device level array to the host and release it."""
         host = np.empty(V, dtype=np.int32)
@@ -433,7 +476,7 @@ class Server:
 
     def free(self) -> None:
         if self._h:
-            lib.xbfs_serve_free(self._h)
+            lib.xbfs_serve_free(self._h)   # stops the online thread first
             self._h = C.c_void_p()
 
     def __del__(self):

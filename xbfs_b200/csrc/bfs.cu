@@ -142,6 +142,9 @@ struct Params {
   int resume;
   int bu_mode;       // bottom-up neighbour probe shape (see probe_range)
   int absent_block;  // failure-detection test hook: CTA absent_block-1 leaves at once
+  int fresh;         // 1: the launch sets up the traversal from src itself (init_traversal)
+  int src;
+  const uint32_t* iso;  // isolated-vertex bitmap: the initial visited set
 };
 
 __device__ __forceinline__ int bin_of(long long d, int small_max, int medium_max) {
@@ -1088,6 +1091,66 @@ __device__ void clear_bitmap(uint32_t* bm, long long nw) {
   for (long long w = w0 + threadIdx.x; w < w1; w += kBlock) bm[w] = 0u;
 }
 
+// Fills n int32 with val; the 16-byte aligned body is split evenly between
+// the CTAs and written with vector stores, CTA 0 also writes the unaligned
+// head and tail (the array is 4-byte aligned).
+__device__ void fill_i32(int* a, long long n, int val) {
+  const long long G = gridDim.x, b = blockIdx.x;
+  long long head = (long long)(((16u - ((unsigned)(uintptr_t)a & 15u)) & 15u) >> 2);
+  if (head > n) head = n;
+  const long long body = (n - head) >> 2;
+  const long long tail = head + body * 4;
+  int4* b4 = reinterpret_cast<int4*>(a + head);
+  const int4 v4 = make_int4(val, val, val, val);
+  for (long long i = body * b / G + threadIdx.x, i1 = body * (b + 1) / G; i < i1; i += kBlock) b4[i] = v4;
+  if (b == 0) {
+    if (threadIdx.x < head) a[threadIdx.x] = val;
+    if (tail + threadIdx.x < n) a[tail + threadIdx.x] = val;
+  }
+}
+
+// Set-up of a traversal from p.src inside the traversal launch (the host
+// only zeroes the control block): levels (and parents) -1, visited = the
+// isolated vertices plus the source, frontier bitmaps empty but for the
+// source's bit in level 0's, and, by CTA 0, the source's queue entry and
+// level 0's frontier descriptor. Every word is written by one thread only,
+// so the source's bits are part of the copy, not a second write; the
+// source's own level and parent are written after the grid barrier that
+// follows (the traversal never reads the level array).
+template <bool PAR>
+__device__ void init_traversal(const Params& p) {
+  fill_i32(p.levels, p.V, -1);
+  if (PAR) fill_i32(p.parents, p.V, -1);
+  const long long G = gridDim.x, b = blockIdx.x;
+  const long long nw = p.nwords;
+  const long long sw = p.src >> 5;
+  const uint32_t sbit = 1u << (p.src & 31);
+  // the bitmaps' 64 padding words past V (all-visited in iso) go to the last CTA
+  const long long w0 = nw * b / G, w1 = (b == G - 1) ? nw + 64 : nw * (b + 1) / G;
+  for (long long w = w0 + threadIdx.x; w < w1; w += kBlock) {
+    const uint32_t own = (w == sw) ? sbit : 0u;
+    p.vis[w] = p.iso[w] | own;
+    p.fb[0][w] = own;
+    p.fb[1][w] = 0u;
+    p.fb[2][w] = 0u;
+    p.fb[3][w] = 0u;
+  }
+  if (b == 0 && threadIdx.x == 0) {
+    const long long b0 = p.beg[p.src];
+    const long long d = p.beg[p.src + 1] - b0;
+    FDesc& f = p.ctl->fd[0];
+    f.n = 1;
+    f.m = (unsigned long long)d;
+    if (d > 0) {
+      const int bin = bin_of(d, p.small_max, p.medium_max);
+      p.q[0][bin].ids[0] = p.src;
+      p.q[0][bin].eb[0] = 0;
+      p.q[0][bin].bg[0] = b0;
+      f.bin[bin] = ((unsigned long long)d << 31) | 1ull;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // The persistent traversal kernel.
 // ---------------------------------------------------------------------------
@@ -1136,6 +1199,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
   const uint32_t nb = gridDim.x;
   uint32_t epoch = 0;
   long long L = 0;
+  if (p.fresh) {
+    init_traversal<PAR>(p);
+    if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      p.levels[p.src] = 0;
+      if (PAR) p.parents[p.src] = p.src;
+    }
+  }
   if (p.resume) {
     const ResumeState r = *p.rs;
     L = r.L;
@@ -1478,6 +1549,8 @@ static xbfs_status setup_params(Graph* g, const xbfs_opts& o, int* d_levels, int
   p.bu_mode = o.bu_probe;
   p.stop_level = LLONG_MAX;
   p.resume = 0;
+  p.fresh = 0;
+  p.iso = g->iso.as<uint32_t>();
   *kfn_out = kfn;
   *smem_out = smem;
   *grid_out = grid;
@@ -1560,9 +1633,13 @@ xbfs_status bfs_single(Graph* g, int32_t src, int32_t* levels, int32_t* parents,
   if ((st = setup_params(g, o, d_levels, d_parents, p, &kfn, &smem, &grid))) return st;
   const bool par_on = parents != nullptr;
 
-  // ---- initial state
+  // ---- one launch: it sets up the traversal state itself (init_traversal);
+  // only the control block, which holds the launch's grid barrier, is
+  // zeroed beforehand
   XBFS_CUDA_TRY(cudaEventRecord(w.ev0, s));
-  if ((st = init_state(g, p, src, par_on, s))) return st;
+  XBFS_CUDA_TRY(cudaMemsetAsync(p.ctl, 0, sizeof(Ctl), s));
+  p.fresh = 1;
+  p.src = src;
   void* args[] = {&p};
   XBFS_CUDA_TRY(cudaEventRecord(w.evk0, s));
   XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, smem, s));
@@ -1674,6 +1751,11 @@ xbfs_status bfs_many(Graph* g, const int32_t* srcs, int32_t n, int32_t* levels, 
   if ((st = setup_params(g, o, dev_out ? levels : dbuf[0], nullptr, p, &kfn, &smem, &grid))) return st;
 
   XBFS_CUDA_TRY(cudaEventRecord(w.ev0, s));
+  // every traversal has its own control block (grid barrier, descriptors,
+  // results), all zeroed here at once, so a traversal is a single launch
+  Ctl* ctls = w.ctl_log.as<Ctl>();
+  XBFS_CUDA_TRY(cudaMemsetAsync(ctls, 0, sizeof(Ctl) * (size_t)n, s));
+  p.fresh = 1;
   auto copy_out = [&](int i) -> xbfs_status {
     const int b = i & 1;
     XBFS_CUDA_TRY(cudaStreamWaitEvent(w.copy_stream, w.ev_done[b], 0));
@@ -1690,10 +1772,10 @@ xbfs_status bfs_many(Graph* g, const int32_t* srcs, int32_t n, int32_t* levels, 
       p.levels = dbuf[b];
       if (i >= 2) XBFS_CUDA_TRY(cudaStreamWaitEvent(s, w.ev_copied[b], 0));  // buffer copied out
     }
-    if ((st = init_state(g, p, srcs[i], false, s))) return st;
+    p.src = srcs[i];
+    p.ctl = ctls + i;
     void* args[] = {&p};
     XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, smem, s));
-    XBFS_CUDA_TRY(cudaMemcpyAsync(w.ctl_log.as<Ctl>() + i, p.ctl, sizeof(Ctl), cudaMemcpyDeviceToDevice, s));
     if (!dev_out) {
       XBFS_CUDA_TRY(cudaEventRecord(w.ev_done[b], s));
       // the copy of the previous traversal is issued after this launch, so
@@ -2120,17 +2202,15 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
   int grid = dev->grid[par_on ? 1 : 0][mlp_on ? 1 : 0];
   if (o.grid_dim > 0 && o.grid_dim < grid) grid = o.grid_dim;
 
-  // ---- initial state (the same steps as init_state) and the launch
+  // ---- the launch sets up the traversal state itself (init_traversal);
+  // the control block, which holds its grid barrier, is zeroed first
   cudaStream_t s = o.stream ? (cudaStream_t)o.stream : g->stream;
-  XBFS_CUDA_TRY(cudaMemsetAsync(p.levels, 0xff, (size_t)g->V * 4, s));
-  if (par_on) XBFS_CUDA_TRY(cudaMemsetAsync(p.parents, 0xff, (size_t)g->V * 4, s));
-  XBFS_CUDA_TRY(cudaMemcpyAsync(p.vis, g->iso.p, nw * 4, cudaMemcpyDeviceToDevice, s));
-  XBFS_CUDA_TRY(cudaMemsetAsync(p.fb[0], 0, nw * 4 * 4, s));
   XBFS_CUDA_TRY(cudaMemsetAsync(p.ctl, 0, sizeof(Ctl), s));
   if (o.policy == XBFS_POLICY_FORCED)
     XBFS_CUDA_TRY(cudaMemcpyAsync((void*)p.forced, o.forced, (size_t)o.n_forced, cudaMemcpyHostToDevice, s));
-  k_seed<<<1, 32, 0, s>>>(p, src, par_on ? 1 : 0);
-  XBFS_CUDA_TRY(cudaGetLastError());
+  p.fresh = 1;
+  p.src = src;
+  p.iso = g->iso.as<uint32_t>();
   void* args[] = {&p};
   XBFS_CUDA_TRY(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kBlock), args, smem, s));
   Ctl hctl;

@@ -28,8 +28,12 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <deque>
 #include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -462,16 +466,34 @@ __global__ void k_sv_clear(Params p, unsigned long long mask) {
 
 }  // namespace sv
 
+// ---------------------------------------------------------------------------
+// Host side: the serving engine. One step (engine_step) processes the rounds
+// that have ended (finished slots leave, their outputs are freed, kept or
+// copied out), admits waiting requests into free slots within the HBM
+// budget, and issues the next round of every batch with work. Two drivers
+// share it: xbfs_serve_run replays a request trace in the caller's thread,
+// and the online mode runs it in the server's own host thread, fed by
+// xbfs_serve_submit and read by xbfs_serve_poll.
+// ---------------------------------------------------------------------------
 struct ServeRequest {
-  int graph;
-  int src;
-  double arrival_us;
+  int graph = 0;
+  int src = 0;
+  double arrival_us = 0;
   double admit_us = -1, finish_us = -1;
   int slot = -1;
-  int* out = nullptr;     // device output (int32[V])
+  int* out = nullptr;          // device output (int32[V])
   long long join = 0;
-  int status = 0;         // 0 waiting, 1 running, 2 done
+  int status = 0;              // 0 waiting, 1 running, 3 copying out, 2 done, 4 dropped at stop
   unsigned long long msum = 0;
+  int mode = 0;                // output: 0 freed at completion, 1 kept on the device, 2 copied to host_out
+  int32_t* host_out = nullptr;
+};
+
+// Finished requests whose levels are being copied to host arrays; done when
+// the event (recorded after the copies) has passed.
+struct Delivery {
+  cudaEvent_t ev = nullptr;
+  std::vector<int> reqs;
 };
 
 struct SlotBatch {
@@ -484,31 +506,48 @@ struct SlotBatch {
   unsigned long long busy = 0;
   std::deque<int> waiting;
   int k_ticks = 1;
+  int depth_est = 0;             // largest depth of a request finished on this graph (0: none yet)
   int grid = 0;
   int max_coop = 0;              // blocks of k_sv_round that can be resident at once
   bool inflight = false;         // a round of ticks is on the stream
   int round_k = 0;               // its length
   long long issued = 0;          // first tick not yet issued
   cudaEvent_t ev = nullptr;      // end of the round in flight
+  std::deque<Delivery> deliveries;
+  std::vector<cudaEvent_t> spare;  // delivery events for reuse
 };
+
+// Traversals at least this deep mark a long-diameter graph: its rounds are
+// sized from the frontier (a few SMs), since its frontier grows slowly.
+constexpr int kDeepGraph = 256;
 
 struct Server {
   int device = 0;
   std::vector<std::unique_ptr<SlotBatch>> batches;
   size_t budget = 0, in_use = 0;
   cudaMemPool_t pool = nullptr;
-  std::vector<ServeRequest> reqs;
-  ~Server() {
-    DeviceGuard dg(device);
-    for (auto& b : batches) {
-      if (b->stream) {
-        cudaStreamSynchronize(b->stream);
-        cudaStreamDestroy(b->stream);
-      }
-      if (b->ev) cudaEventDestroy(b->ev);
-    }
-  }
+  // requests of the current replay, or every request submitted online
+  // (a deque: references stay valid while requests are appended)
+  std::deque<ServeRequest> reqs;
+  long long done = 0;
+  std::chrono::steady_clock::time_point t0;
+  PinnedBuf hctl_buf;            // control blocks read back after each round
+  // online mode
+  bool online = false;
+  bool stop = false;
+  std::thread worker;
+  std::mutex mu;                 // guards everything above while online
+  std::condition_variable cv;    // submissions, completions, releases, failure
+  std::vector<int> inbox;        // submitted requests not yet queued to their batch
+  cudaStream_t release_stream = nullptr;  // frees of kept level arrays (xbfs_serve_release)
+  xbfs_status failed = XBFS_OK;  // the worker's error, if it stopped on one
+  std::string fail_msg;
+  ~Server();
 };
+
+static double now_us(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+}
 
 static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
   b.g = g;
@@ -552,7 +591,33 @@ static xbfs_status batch_init(SlotBatch& b, Graph* g, int nsm) {
   if (per_sm < 1) return set_error(XBFS_ERR_INTERNAL, "serving round kernel cannot be resident");
   b.max_coop = nsm * per_sm;
   b.grid = b.max_coop;
+  XBFS_CUDA_TRY(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming));
   return XBFS_OK;
+}
+
+Server::~Server() {
+  if (worker.joinable()) {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+    }
+    cv.notify_all();
+    worker.join();
+  }
+  DeviceGuard dg(device);
+  for (auto& b : batches) {
+    if (b->stream) {
+      cudaStreamSynchronize(b->stream);
+      cudaStreamDestroy(b->stream);
+    }
+    if (b->ev) cudaEventDestroy(b->ev);
+    for (auto& d : b->deliveries) cudaEventDestroy(d.ev);
+    for (cudaEvent_t e : b->spare) cudaEventDestroy(e);
+  }
+  if (release_stream) {
+    cudaStreamSynchronize(release_stream);
+    cudaStreamDestroy(release_stream);
+  }
 }
 
 // Issues k ticks on the batch's stream with `grid` blocks per tick kernel
@@ -572,8 +637,256 @@ static xbfs_status batch_ticks(SlotBatch& b, int k, int grid) {
   return XBFS_OK;
 }
 
-static double now_us(std::chrono::steady_clock::time_point t0) {
-  return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+// Marks a request done (the caller notifies waiters).
+static void finish_request(Server* srv, ServeRequest& r, double t) {
+  r.finish_us = t;
+  r.status = 2;
+  srv->done += 1;
+}
+
+// One step of the engine; *active is set when anything is waiting, running
+// or being copied out (so the driver keeps stepping). `oom_is_error`: a
+// waiting request that only kept outputs block, with nothing running, is an
+// XBFS_ERR_OOM (replay) instead of a wait for xbfs_serve_release (online).
+static xbfs_status engine_step(Server* srv, bool oom_is_error, bool* active, bool* progressed) {
+  const int nb = (int)srv->batches.size();
+  sv::Ctl* hctl = srv->hctl_buf.as<sv::Ctl>();
+  *progressed = false;
+  // ---- copies to host arrays that have completed
+  for (int gi = 0; gi < nb; ++gi) {
+    SlotBatch& b = *srv->batches[gi];
+    while (!b.deliveries.empty()) {
+      Delivery& d = b.deliveries.front();
+      const cudaError_t q = cudaEventQuery(d.ev);
+      if (q == cudaErrorNotReady) break;
+      XBFS_CUDA_TRY(q);
+      const double t = now_us(srv->t0);
+      for (int ri : d.reqs) finish_request(srv, srv->reqs[ri], t);
+      b.spare.push_back(d.ev);
+      b.deliveries.pop_front();
+      *progressed = true;
+    }
+  }
+  // ---- rounds that have ended: the slots that gained nothing at some tick
+  for (int gi = 0; gi < nb; ++gi) {
+    SlotBatch& b = *srv->batches[gi];
+    if (!b.inflight) continue;
+    const cudaError_t q = cudaEventQuery(b.ev);
+    if (q == cudaErrorNotReady) continue;
+    XBFS_CUDA_TRY(q);
+    b.inflight = false;
+    *progressed = true;
+    if (hctl[gi].bar.err != 0)
+      return set_error((xbfs_status)hctl[gi].bar.err, "serving round on graph %d reported %s", gi,
+                       xbfs_strerror(hctl[gi].bar.err));
+    const int k = b.round_k;
+    unsigned long long finished = 0;
+    for (int i = 0; i < k; ++i) {
+      const long long t = b.tick + i;
+      const unsigned long long act = hctl[gi].active[t % sv::kRing];
+      // slots joined at or before t that gained nothing at t are complete
+      for (unsigned long long m = b.busy & ~finished; m; m &= m - 1) {
+        const int sl = __builtin_ctzll(m);
+        const ServeRequest& r = srv->reqs[b.req_of_slot[sl]];
+        if (r.join <= t && !((act >> sl) & 1ull)) finished |= 1ull << sl;
+      }
+    }
+    b.tick += k;
+    if (!finished) {
+      // longer rounds while nothing finishes, but never beyond an eighth of
+      // the depth seen on this graph (a low-diameter graph keeps short rounds,
+      // so the host notices its completions within a tick or two)
+      if (b.depth_est == 0 || b.k_ticks * 8 < b.depth_est) b.k_ticks = std::min(sv::kRing, b.k_ticks * 2);
+      continue;
+    }
+    const double tf = now_us(srv->t0);
+    int max_depth = 0;
+    // the slots leave the tables (k_sv_clear) before their arrays are freed
+    sv::k_sv_clear<<<b.grid, 256, 0, b.stream>>>(b.p, finished);
+    XBFS_CUDA_TRY(cudaGetLastError());
+    Delivery dl;
+    for (unsigned long long m = finished; m; m &= m - 1) {
+      const int sl = __builtin_ctzll(m);
+      const int ri = b.req_of_slot[sl];
+      ServeRequest& r = srv->reqs[ri];
+      r.msum = hctl[gi].msum[sl];
+      max_depth = std::max<int>(max_depth, (int)(b.tick - r.join));
+      if (r.mode == 2) {  // copy to the caller's host array, then give the memory back
+        XBFS_CUDA_TRY(cudaMemcpyAsync(r.host_out, r.out, (size_t)b.g->V * 4, cudaMemcpyDeviceToHost, b.stream));
+        dl.reqs.push_back(ri);
+        r.status = 3;
+      }
+      if (r.mode != 1) {
+        XBFS_CUDA_TRY(cudaFreeAsync(r.out, b.stream));
+        srv->in_use -= (size_t)b.g->V * 4;
+        r.out = nullptr;
+      }
+      if (r.mode != 2) finish_request(srv, r, tf);
+      b.req_of_slot[sl] = -1;
+    }
+    if (!dl.reqs.empty()) {
+      if (b.spare.empty()) {
+        cudaEvent_t e;
+        XBFS_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b.spare.push_back(e);
+      }
+      dl.ev = b.spare.back();
+      b.spare.pop_back();
+      XBFS_CUDA_TRY(cudaEventRecord(dl.ev, b.stream));
+      b.deliveries.push_back(std::move(dl));
+    }
+    b.busy &= ~finished;
+    b.depth_est = std::max(b.depth_est, max_depth);
+    // host every ~1/8 of the depth seen so far, at least every tick
+    b.k_ticks = std::max(1, std::min(sv::kRing, b.depth_est / 8));
+  }
+  // ---- admission: a free slot and room in the HBM budget; a request joins
+  // at the batch's next unissued tick (its seed is stream-ordered after the
+  // round in flight)
+  for (int gi = 0; gi < nb; ++gi) {
+    SlotBatch& b = *srv->batches[gi];
+    while (!b.waiting.empty() && b.busy != ~0ull) {
+      const size_t need = (size_t)b.g->V * 4;
+      if (srv->in_use + need > srv->budget) break;
+      const int ri = b.waiting.front();
+      b.waiting.pop_front();
+      ServeRequest& r = srv->reqs[ri];
+      const int sl = __builtin_ctzll(~b.busy);
+      b.busy |= 1ull << sl;
+      b.req_of_slot[sl] = ri;
+      void* mem = nullptr;
+      XBFS_CUDA_TRY(cudaMallocFromPoolAsync(&mem, need, srv->pool, b.stream));
+      srv->in_use += need;
+      r.out = (int*)mem;
+      r.slot = sl;
+      r.join = b.issued;
+      r.admit_us = now_us(srv->t0);
+      r.status = 1;
+      XBFS_CUDA_TRY(cudaMemsetAsync(r.out, 0xff, need, b.stream));
+      // the seed goes into tick b.issued's frontier and records the slot's
+      // output array and join tick
+      sv::k_sv_seed<<<1, 32, 0, b.stream>>>(b.p, b.issued, sl, r.src, r.out);
+      XBFS_CUDA_TRY(cudaGetLastError());
+      *progressed = true;
+    }
+  }
+  // ---- the next round of every idle batch with running slots; the
+  // resident-block budget of the device is split between the batches that
+  // have work, so that their cooperative rounds can be resident together
+  // (a round needing the whole device would wait for every other to end)
+  int with_work = 0;
+  for (int gi = 0; gi < nb; ++gi) with_work += srv->batches[gi]->busy ? 1 : 0;
+  bool any = false;
+  for (int gi = 0; gi < nb; ++gi) {
+    SlotBatch& b = *srv->batches[gi];
+    if (!b.waiting.empty() || !b.deliveries.empty()) any = true;
+    if (b.inflight) {
+      any = true;
+      continue;
+    }
+    if (!b.busy) continue;
+    any = true;
+    const int k = std::max(1, std::min(b.k_ticks, sv::kRing - (int)(b.tick % sv::kRing)));
+    // Blocks of the round: on a long-diameter graph (deep traversals seen)
+    // from the frontier the round starts with, with 4x headroom for growth
+    // inside the round, so such batches use a few SMs and share the GPU
+    // instead of taking turns. Low-diameter graphs, whose frontier can grow a
+    // thousandfold in one tick, and graphs not yet seen to be deep get every
+    // resident block of their share.
+    int grid = b.grid;
+    if (b.tick > 0 && b.depth_est >= kDeepGraph) {
+      const unsigned long long pk = hctl[gi].q[b.tick % 4];
+      const unsigned long long work = std::max<unsigned long long>(pk >> 31, pk & sv::kCountMask);
+      const unsigned long long want = (work * 4 + sv::kBlock * 2 - 1) / (sv::kBlock * 2);
+      grid = (int)std::min<unsigned long long>((unsigned long long)b.grid, std::max<unsigned long long>(8, want));
+    }
+    grid = std::min(grid, std::max(8, b.max_coop / std::max(1, with_work)));
+    xbfs_status st = batch_ticks(b, k, grid);
+    if (st) return st;
+    XBFS_CUDA_TRY(cudaMemcpyAsync(&hctl[gi], b.ctl.p, sizeof(sv::Ctl), cudaMemcpyDeviceToHost, b.stream));
+    XBFS_CUDA_TRY(cudaEventRecord(b.ev, b.stream));
+    b.round_k = k;
+    b.issued = b.tick + k;
+    b.inflight = true;
+    *progressed = true;
+  }
+  bool running = false;
+  for (int gi = 0; gi < nb; ++gi) running |= srv->batches[gi]->inflight || !srv->batches[gi]->deliveries.empty();
+  if (!running && oom_is_error) {
+    // nothing runs, so nothing will give memory back: a request that waits
+    // can only be blocked by kept outputs
+    for (int gi = 0; gi < nb; ++gi)
+      if (!srv->batches[gi]->waiting.empty())
+        return set_error(XBFS_ERR_OOM,
+                         "kept level arrays (%zu bytes) fill the HBM budget (%zu bytes): release them, or run "
+                         "with keep_outputs = 0 or 2",
+                         srv->in_use, srv->budget);
+  }
+  *active = any;
+  return XBFS_OK;
+}
+
+// Prepares a server for a run of requests (replay or online): fresh clock,
+// per-batch round state, the pinned read-back buffer.
+static xbfs_status engine_reset(Server* srv) {
+  const int nb = (int)srv->batches.size();
+  if (xbfs_status st = srv->hctl_buf.ensure(sizeof(sv::Ctl) * (size_t)nb)) return st;
+  for (auto& bp : srv->batches) {
+    bp->inflight = false;
+    bp->issued = bp->tick;
+  }
+  srv->reqs.clear();
+  srv->done = 0;
+  srv->t0 = std::chrono::steady_clock::now();
+  return XBFS_OK;
+}
+
+// The online worker: hands submitted requests to their batches and steps
+// the engine while there is work; sleeps on the condition variable when
+// idle. Holds the mutex except while idle or yielding between steps.
+static void worker_main(Server* srv) {
+  cudaSetDevice(srv->device);
+  std::unique_lock<std::mutex> lk(srv->mu);
+  for (;;) {
+    for (int ri : srv->inbox) srv->batches[srv->reqs[ri].graph]->waiting.push_back(ri);
+    srv->inbox.clear();
+    bool active = false, progressed = false;
+    const long long done_before = srv->done;
+    const xbfs_status st = engine_step(srv, false, &active, &progressed);
+    if (st) {
+      srv->failed = st;
+      srv->fail_msg = xbfs_last_error();
+      srv->cv.notify_all();
+      return;
+    }
+    if (srv->done != done_before) srv->cv.notify_all();
+    if (!active) {
+      if (srv->stop) return;
+      srv->cv.wait(lk, [&] { return !srv->inbox.empty() || srv->stop; });
+      continue;
+    }
+    if (progressed) continue;
+    bool running = false;
+    for (auto& b : srv->batches) running |= b->inflight || !b->deliveries.empty();
+    if (running) {
+      // rounds in flight: let submitters and pollers in, then poll again
+      lk.unlock();
+      std::this_thread::yield();
+      lk.lock();
+    } else if (srv->stop) {
+      // only requests that kept outputs block remain, and nothing will run
+      // to free memory: they are dropped
+      for (auto& b : srv->batches) {
+        for (int ri : b->waiting) srv->reqs[ri].status = 4;
+        b->waiting.clear();
+      }
+      srv->cv.notify_all();
+      return;
+    } else {
+      // waiting requests that kept outputs block: a release wakes the worker
+      srv->cv.wait_for(lk, std::chrono::milliseconds(1));
+    }
+  }
 }
 
 }  // namespace xbfs
@@ -607,6 +920,7 @@ xbfs_status xbfs_serve_create(xbfs_graph* const* graphs, int32_t n, int32_t devi
   XBFS_CUDA_TRY(cudaDeviceGetDefaultMemPool(&srv->pool, device));
   uint64_t thr = UINT64_MAX;
   XBFS_CUDA_TRY(cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  XBFS_CUDA_TRY(cudaStreamCreateWithFlags(&srv->release_stream, cudaStreamNonBlocking));
   XBFS_CUDA_TRY(cudaDeviceSynchronize());
   *out = (xbfs_server*)srv.release();
   return XBFS_OK;
@@ -626,6 +940,7 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
   if (!srv || n < 0 || (n > 0 && (!graph || !src || !arrival_us || !admit_us || !finish_us))) {
     return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
   }
+  if (srv->online) return set_error(XBFS_ERR_BUSY, "the server runs online (xbfs_serve_start): stop it first");
   if (keep_outputs < 0 || keep_outputs > 2) return set_error(XBFS_ERR_INVALID_ARG, "keep_outputs must be 0, 1 or 2");
   if (keep_outputs && !levels) return set_error(XBFS_ERR_INVALID_ARG, "keep_outputs needs levels[]");
   if (keep_outputs == 2)
@@ -633,190 +948,51 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
       if (!levels[i]) return set_error(XBFS_ERR_INVALID_ARG, "request %d: no host level array", i);
   DeviceGuard dg(srv->device);
   const int nb = (int)srv->batches.size();
-  srv->reqs.assign(n, ServeRequest());
-  std::vector<int> order(n);
   for (int i = 0; i < n; ++i) {
     if (graph[i] < 0 || graph[i] >= nb) return set_error(XBFS_ERR_INVALID_ARG, "request %d: bad graph", i);
     if (src[i] < 0 || src[i] >= srv->batches[graph[i]]->g->V)
       return set_error(XBFS_ERR_INVALID_ARG, "request %d: source out of range", i);
-    srv->reqs[i].graph = graph[i];
-    srv->reqs[i].src = src[i];
-    srv->reqs[i].arrival_us = arrival_us[i];
-    order[i] = i;
-  }
-  for (int i = 0; i < n; ++i)
     if ((size_t)srv->batches[graph[i]]->g->V * 4 > srv->budget)
       return set_error(XBFS_ERR_OOM, "request %d: its level array does not fit the HBM budget", i);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return arrival_us[a] < arrival_us[b]; });
-  const auto t0 = std::chrono::steady_clock::now();
-  size_t next = 0;
-  int done = 0;
-  // every batch advances in rounds of up to kRing ticks; a round is issued,
-  // its end marked by an event, and processed when that event has passed, so
-  // a batch with short traversals is never held up by one with long ones
-  PinnedBuf hctl_buf;
-  if (xbfs_status st = hctl_buf.ensure(sizeof(sv::Ctl) * (size_t)nb)) return st;
-  sv::Ctl* hctl = hctl_buf.as<sv::Ctl>();
-  for (auto& bp : srv->batches) {
-    bp->inflight = false;
-    bp->issued = bp->tick;
-    if (!bp->ev) XBFS_CUDA_TRY(cudaEventCreateWithFlags(&bp->ev, cudaEventDisableTiming));
   }
+  if (xbfs_status st = engine_reset(srv)) return st;
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) {
+    ServeRequest r;
+    r.graph = graph[i];
+    r.src = src[i];
+    r.arrival_us = arrival_us[i];
+    r.mode = keep_outputs;
+    r.host_out = keep_outputs == 2 ? levels[i] : nullptr;
+    srv->reqs.push_back(r);
+    order[i] = i;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return arrival_us[a] < arrival_us[b]; });
+  size_t next = 0;
   const double last_arrival = n ? srv->reqs[order.back()].arrival_us : 0.0;
-  while (done < n) {
-    const double now = now_us(t0);
+  while (srv->done < n) {
+    const double now = now_us(srv->t0);
     if (now > last_arrival + 1200e6)
       return set_error(XBFS_ERR_DEVICE_TIMEOUT, "serving loop made no progress for 20 minutes");
-    // arrivals
     while (next < order.size() && srv->reqs[order[next]].arrival_us <= now) {
       srv->batches[srv->reqs[order[next]].graph]->waiting.push_back(order[next]);
       ++next;
     }
-    // completed rounds: find the slots that gained nothing at some tick
-    for (int gi = 0; gi < nb; ++gi) {
-      SlotBatch& b = *srv->batches[gi];
-      if (!b.inflight) continue;
-      const cudaError_t q = cudaEventQuery(b.ev);
-      if (q == cudaErrorNotReady) continue;
-      XBFS_CUDA_TRY(q);
-      b.inflight = false;
-      if (hctl[gi].bar.err != 0)
-        return set_error((xbfs_status)hctl[gi].bar.err, "serving round on graph %d reported %s", gi,
-                         xbfs_strerror(hctl[gi].bar.err));
-      const int k = b.round_k;
-      unsigned long long finished = 0;
-      for (int i = 0; i < k; ++i) {
-        const long long t = b.tick + i;
-        const unsigned long long act = hctl[gi].active[t % sv::kRing];
-        // slots joined at or before t that gained nothing at t are complete
-        for (unsigned long long m = b.busy & ~finished; m; m &= m - 1) {
-          const int sl = __builtin_ctzll(m);
-          const ServeRequest& r = srv->reqs[b.req_of_slot[sl]];
-          if (r.join <= t && !((act >> sl) & 1ull)) finished |= 1ull << sl;
-        }
-      }
-      b.tick += k;
-      if (!finished) {
-        b.k_ticks = std::min(sv::kRing, b.k_ticks * 2);
-        continue;
-      }
-      const double tf = now_us(t0);
-      int max_depth = 0;
-      // the slots leave the tables (k_sv_clear) before their arrays are freed
-      sv::k_sv_clear<<<b.grid, 256, 0, b.stream>>>(b.p, finished);
-      XBFS_CUDA_TRY(cudaGetLastError());
-      for (unsigned long long m = finished; m; m &= m - 1) {
-        const int sl = __builtin_ctzll(m);
-        ServeRequest& r = srv->reqs[b.req_of_slot[sl]];
-        r.finish_us = tf;
-        r.status = 2;
-        r.msum = hctl[gi].msum[sl];
-        max_depth = std::max<int>(max_depth, (int)(b.tick - r.join));
-        if (keep_outputs == 2)  // deliver to the caller's host array, then give the memory back
-          XBFS_CUDA_TRY(cudaMemcpyAsync(levels[b.req_of_slot[sl]], r.out, (size_t)b.g->V * 4, cudaMemcpyDeviceToHost,
-                                        b.stream));
-        if (keep_outputs != 1) {
-          XBFS_CUDA_TRY(cudaFreeAsync(r.out, b.stream));
-          srv->in_use -= (size_t)b.g->V * 4;
-          r.out = nullptr;
-        }
-        b.req_of_slot[sl] = -1;
-        ++done;
-      }
-      b.busy &= ~finished;
-      // host every ~1/8 of the depth seen so far, at least every tick
-      b.k_ticks = std::max(1, std::min(sv::kRing, max_depth / 8));
-    }
-    // admission: a free slot and room in the HBM budget; a request joins at
-    // the batch's next unissued tick (its seed is stream-ordered after the
-    // round in flight)
-    for (int gi = 0; gi < nb; ++gi) {
-      SlotBatch& b = *srv->batches[gi];
-      while (!b.waiting.empty() && b.busy != ~0ull) {
-        const size_t need = (size_t)b.g->V * 4;
-        if (srv->in_use + need > srv->budget) break;
-        const int ri = b.waiting.front();
-        b.waiting.pop_front();
-        ServeRequest& r = srv->reqs[ri];
-        const int sl = __builtin_ctzll(~b.busy);
-        b.busy |= 1ull << sl;
-        b.req_of_slot[sl] = ri;
-        void* mem = nullptr;
-        XBFS_CUDA_TRY(cudaMallocFromPoolAsync(&mem, need, srv->pool, b.stream));
-        srv->in_use += need;
-        r.out = (int*)mem;
-        r.slot = sl;
-        r.join = b.issued;
-        r.admit_us = now_us(t0);
-        r.status = 1;
-        XBFS_CUDA_TRY(cudaMemsetAsync(r.out, 0xff, need, b.stream));
-        // the seed goes into tick b.issued's frontier and records the slot's
-        // output array and join tick
-        sv::k_sv_seed<<<1, 32, 0, b.stream>>>(b.p, b.issued, sl, r.src, r.out);
-        XBFS_CUDA_TRY(cudaGetLastError());
-      }
-    }
-    // issue the next round of every idle batch with running slots; the
-    // resident-block budget of the device is split between the batches that
-    // have work, so that their cooperative rounds can be resident together
-    // (a round needing the whole device would wait for every other to end)
-    int with_work = 0;
-    for (int gi = 0; gi < nb; ++gi) with_work += srv->batches[gi]->busy ? 1 : 0;
-    int running = 0;
-    for (int gi = 0; gi < nb; ++gi) {
-      SlotBatch& b = *srv->batches[gi];
-      if (b.inflight) {
-        ++running;
-        continue;
-      }
-      if (!b.busy) continue;
-      ++running;
-      const int k = std::max(1, std::min(b.k_ticks, sv::kRing - (int)(b.tick % sv::kRing)));
-      // Blocks of the round from the frontier it starts with (4x headroom for
-      // growth inside the round) when the rounds are long, i.e. the graph's
-      // traversals are deep and their frontiers grow slowly: those batches
-      // then use a few SMs and share the GPU instead of taking turns. Short
-      // rounds (low-diameter graphs, whose frontier can grow a thousandfold
-      // in one tick) get every resident block.
-      int grid = b.grid;
-      if (b.tick > 0 && k >= 16) {  // long rounds: the frontier grows slowly (long-diameter graphs)
-        const unsigned long long pk = hctl[gi].q[b.tick % 4];
-        const unsigned long long work = std::max<unsigned long long>(pk >> 31, pk & sv::kCountMask);
-        const unsigned long long want = (work * 4 + sv::kBlock * 2 - 1) / (sv::kBlock * 2);
-        grid = (int)std::min<unsigned long long>((unsigned long long)b.grid, std::max<unsigned long long>(8, want));
-      }
-      grid = std::min(grid, std::max(8, b.max_coop / std::max(1, with_work)));
-      xbfs_status st = batch_ticks(b, k, grid);
-      if (st) return st;
-      XBFS_CUDA_TRY(cudaMemcpyAsync(&hctl[gi], b.ctl.p, sizeof(sv::Ctl), cudaMemcpyDeviceToHost, b.stream));
-      XBFS_CUDA_TRY(cudaEventRecord(b.ev, b.stream));
-      b.round_k = k;
-      b.issued = b.tick + k;
-      b.inflight = true;
-    }
-    if (!running) {
-      // nothing runs, so nothing will give memory back: a request that has
-      // arrived and still waits can only be blocked by kept outputs
-      for (int gi = 0; gi < nb; ++gi)
-        if (!srv->batches[gi]->waiting.empty())
-          return set_error(XBFS_ERR_OOM,
-                           "kept level arrays (%zu bytes) fill the HBM budget (%zu bytes): release them, or run "
-                           "with keep_outputs = 0 or 2",
-                           srv->in_use, srv->budget);
-      if (next < order.size()) {
-        const double wait = srv->reqs[order[next]].arrival_us - now_us(t0);
-        if (wait > 50) {
-          // spin until the next arrival: a sleep would add its wake-up delay
-          // to that request's latency
-          const auto until = t0 + std::chrono::microseconds((long long)srv->reqs[order[next]].arrival_us);
-          while (std::chrono::steady_clock::now() < until) {
-          }
+    bool active = false, progressed = false;
+    if (xbfs_status st = engine_step(srv, true, &active, &progressed)) return st;
+    if (!active && next < order.size()) {
+      const double wait = srv->reqs[order[next]].arrival_us - now_us(srv->t0);
+      if (wait > 50) {
+        // spin until the next arrival: a sleep would add its wake-up delay
+        // to that request's latency
+        const auto until = srv->t0 + std::chrono::microseconds((long long)srv->reqs[order[next]].arrival_us);
+        while (std::chrono::steady_clock::now() < until) {
         }
       }
     }
   }
   for (auto& b : srv->batches) XBFS_CUDA_TRY(cudaStreamSynchronize(b->stream));
-  if (wall_us) *wall_us = now_us(t0);
+  if (wall_us) *wall_us = now_us(srv->t0);
   for (int i = 0; i < n; ++i) {
     admit_us[i] = srv->reqs[i].admit_us;
     finish_us[i] = srv->reqs[i].finish_us;
@@ -826,17 +1002,114 @@ xbfs_status xbfs_serve_run(xbfs_server* sh, int32_t n, const int32_t* graph, con
   return XBFS_OK;
 }
 
+xbfs_status xbfs_serve_start(xbfs_server* sh) {
+  Server* srv = (Server*)sh;
+  if (!srv) return set_error(XBFS_ERR_INVALID_ARG, "server is NULL");
+  if (srv->online) return set_error(XBFS_ERR_BUSY, "the server is already running online");
+  DeviceGuard dg(srv->device);
+  if (xbfs_status st = engine_reset(srv)) return st;
+  srv->stop = false;
+  srv->failed = XBFS_OK;
+  srv->fail_msg.clear();
+  srv->inbox.clear();
+  srv->online = true;
+  try {
+    srv->worker = std::thread(worker_main, srv);
+  } catch (...) {
+    srv->online = false;
+    return set_error(XBFS_ERR_INTERNAL, "cannot start the serving thread");
+  }
+  return XBFS_OK;
+}
+
+xbfs_status xbfs_serve_submit(xbfs_server* sh, int32_t graph, int32_t src, int32_t output, int32_t* levels_host,
+                              int64_t* ticket) {
+  Server* srv = (Server*)sh;
+  if (!srv || !ticket) return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
+  if (output < 0 || output > 2) return set_error(XBFS_ERR_INVALID_ARG, "output must be 0, 1 or 2");
+  if (output == 2 && !levels_host) return set_error(XBFS_ERR_INVALID_ARG, "output 2 needs a host level array");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  if (!srv->online) return set_error(XBFS_ERR_INVALID_ARG, "the server is not running online (xbfs_serve_start)");
+  if (srv->stop) return set_error(XBFS_ERR_BUSY, "the server is stopping");
+  if (srv->failed) return set_error(srv->failed, "serving thread stopped: %s", srv->fail_msg.c_str());
+  const int nb = (int)srv->batches.size();
+  if (graph < 0 || graph >= nb) return set_error(XBFS_ERR_INVALID_ARG, "bad graph %d", graph);
+  if (src < 0 || src >= srv->batches[graph]->g->V) return set_error(XBFS_ERR_INVALID_ARG, "source out of range");
+  if ((size_t)srv->batches[graph]->g->V * 4 > srv->budget)
+    return set_error(XBFS_ERR_OOM, "the level array does not fit the HBM budget");
+  ServeRequest r;
+  r.graph = graph;
+  r.src = src;
+  r.arrival_us = now_us(srv->t0);
+  r.mode = output;
+  r.host_out = output == 2 ? levels_host : nullptr;
+  srv->reqs.push_back(r);
+  const int id = (int)srv->reqs.size() - 1;
+  srv->inbox.push_back(id);
+  *ticket = id;
+  srv->cv.notify_all();
+  return XBFS_OK;
+}
+
+xbfs_status xbfs_serve_poll(xbfs_server* sh, int64_t ticket, int64_t wait_us, xbfs_serve_result* out) {
+  Server* srv = (Server*)sh;
+  if (!srv) return set_error(XBFS_ERR_INVALID_ARG, "server is NULL");
+  std::unique_lock<std::mutex> lk(srv->mu);
+  if (ticket < 0 || ticket >= (int64_t)srv->reqs.size()) return set_error(XBFS_ERR_INVALID_ARG, "unknown ticket");
+  auto ready = [&] { return srv->reqs[ticket].status == 2 || srv->failed != XBFS_OK; };
+  if (!ready() && wait_us != 0) {
+    if (wait_us < 0) srv->cv.wait(lk, ready);
+    else srv->cv.wait_for(lk, std::chrono::microseconds(wait_us), ready);
+  }
+  const ServeRequest& r = srv->reqs[ticket];
+  if (out) {
+    out->struct_size = (int32_t)sizeof(xbfs_serve_result);
+    out->state = r.status == 3 ? 1 : (r.status == 4 ? 3 : r.status);
+    out->submit_us = r.arrival_us;
+    out->admit_us = r.admit_us;
+    out->finish_us = r.finish_us;
+    out->edges_mc = r.status == 2 ? (int64_t)(r.msum / 2) : 0;
+    out->levels_dev = (r.status == 2 && r.mode == 1) ? r.out : nullptr;
+  }
+  if (r.status == 2) return XBFS_OK;
+  if (srv->failed) return set_error(srv->failed, "serving thread stopped: %s", srv->fail_msg.c_str());
+  if (r.status == 4)
+    return set_error(XBFS_ERR_OOM, "request dropped when the server stopped: kept level arrays filled the HBM budget");
+  return XBFS_ERR_BUSY;
+}
+
+xbfs_status xbfs_serve_stop(xbfs_server* sh) {
+  Server* srv = (Server*)sh;
+  if (!srv) return set_error(XBFS_ERR_INVALID_ARG, "server is NULL");
+  if (!srv->online) return XBFS_OK;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->stop = true;
+  }
+  srv->cv.notify_all();
+  if (srv->worker.joinable()) srv->worker.join();
+  DeviceGuard dg(srv->device);
+  for (auto& b : srv->batches) XBFS_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  srv->online = false;
+  if (srv->failed) return set_error(srv->failed, "serving thread stopped: %s", srv->fail_msg.c_str());
+  return XBFS_OK;
+}
+
 xbfs_status xbfs_serve_release(xbfs_server* sh, int32_t* levels_dev, int64_t V) {
   Server* srv = (Server*)sh;
   if (!srv || !levels_dev) return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
   DeviceGuard dg(srv->device);
-  XBFS_CUDA_TRY(cudaFreeAsync(levels_dev, srv->batches[0]->stream));
-  XBFS_CUDA_TRY(cudaStreamSynchronize(srv->batches[0]->stream));
+  std::lock_guard<std::mutex> lk(srv->mu);
+  // stream-ordered free on a stream of its own: no wait for rounds in flight
+  XBFS_CUDA_TRY(cudaFreeAsync(levels_dev, srv->release_stream));
   srv->in_use -= std::min<size_t>(srv->in_use, (size_t)V * 4);
+  for (auto& r : srv->reqs)
+    if (r.out == levels_dev) r.out = nullptr;
+  srv->cv.notify_all();  // room in the budget: the worker may admit again
   return XBFS_OK;
 }
 
-// Copies a kept level array to host memory and releases it.
+// Copies a kept level array to host memory, then releases it.
 xbfs_status xbfs_serve_fetch(xbfs_server* sh, int32_t* levels_dev, int64_t V, int32_t* host_out) {
   Server* srv = (Server*)sh;
   if (!srv || !levels_dev || !host_out || V <= 0) return set_error(XBFS_ERR_INVALID_ARG, "bad arguments");
