@@ -68,3 +68,35 @@ def test_trained_network_gain_over_heuristic():
           f"{r['heuristic']['gteps']:.1f} -> {r['mlp']['gteps']:.1f} GTEPS)")
     assert gain > 1.0
     learned.install(None)
+
+
+@pytest.mark.parametrize("kind", ["grid", "rmat"])
+def test_decisions_are_the_networks_at_every_level(kind):
+    """The kernel evaluates the network only where its last decision could
+    change (certified reuse: the sensitivity bound installed with the
+    weights against the last margin); every level's strategy must still be
+    the network's argmax for that level's features, computed here by the
+    device forward kernel from the trace."""
+    from xbfs_b200 import learned
+    w, _ = learned.load()
+    learned.install(w)
+    try:
+        beg, csr = gen_grid_host(300, 200) if kind == "grid" else gen_rmat_host(16, 16, 4)
+        g = Graph.from_csr(beg, csr)
+        checked = 0
+        for s in pick_sources(beg, 3, 7):
+            r = g.bfs(int(s), policy="mlp", trace=True)
+            assert np.array_equal(r.levels, oracle.bfs_queue(beg, csr, int(s)))
+            tr = r.trace
+            ids = {"td_queue": 0, "td_scan": 1, "bu": 2}
+            rows = [dict(t, strategy_id=ids[t["strategy"]]) for t in tr]
+            lg = learned.logits(w, learned.features_from_trace(rows))
+            for L, t in enumerate(rows):
+                top = np.sort(lg[L])[::-1]
+                if top[0] - top[1] < 1e-3:   # a tie within float noise: either class is the network's
+                    continue
+                assert t["strategy_id"] == int(np.argmax(lg[L])), (kind, int(s), L, lg[L])
+                checked += 1
+        assert checked > 0
+    finally:
+        learned.install(None)

@@ -206,8 +206,9 @@ struct __align__(16) Smem {
   float mlp_raw[8];             // statistics the learned switch's features come from
   float mlp_cache_f[8];         // features of its last evaluation
   int mlp_cache_dec;            // and its decision (-1: none yet)
+  float mlp_cache_margin;       // and that decision's margin
   LoopState ls;
-  float mlp_w[1464];            // the learned switch's weights (XBFS_POLICY_MLP); must stay last
+  float mlp_w[1472];            // the learned switch's weights and bound (XBFS_POLICY_MLP); must stay last
 };
 
 // Loop state carried across launches in stepped mode (xbfs_level_costs): a
@@ -281,9 +282,12 @@ __device__ int decide_beamer(PolicyState& ps, long long n_f, long long m_f, long
 // memory W1 and W2 are stored transposed (input-major), so that lane j
 // reading row j of either walks consecutive banks instead of one bank.
 constexpr int kMlpParams = 16 + 256 + 32 + 1024 + 32 + 96 + 3;  // 1459
+constexpr int kMlpStaged = kMlpParams + 8;  // + the per-feature sensitivity bound set at installation
+
+static_assert(kMlpStaged <= 1472, "the staged weights must fit Smem::mlp_w");
 
 __device__ void mlp_stage(const float* __restrict__ w, float* sw) {
-  for (int t = threadIdx.x; t < kMlpParams; t += blockDim.x) {
+  for (int t = threadIdx.x; t < kMlpStaged; t += blockDim.x) {
     int d = t;
     if (t >= 16 && t < 16 + 256) {  // W1[j][i] -> W1T[i][j]
       const int j = (t - 16) / 8, i = (t - 16) % 8;
@@ -300,15 +304,17 @@ __device__ void mlp_stage(const float* __restrict__ w, float* sw) {
 // strategy; log growth of the frontier; log1p of its mean degree), one per
 // lane, then the three layers with the hidden activations passed by shuffles.
 // Called by one full warp.
-// Inference cache (per CTA, in shared memory): when every normalised feature
-// is within kMlpReuse of the ones the network last saw, that decision is
-// reused. Long runs of nearly identical levels (a grid's ring of a few
-// thousand vertices growing by a few per level) then skip the layers;
-// levels where the frontier changes by more than a few percent always
-// evaluate the network.
-constexpr float kMlpReuse = 0.02f;
-
-__device__ int mlp_decide(const float* sw, const float* raw, int lane, float* cache_f, int* cache_dec) {
+// Certified reuse (per CTA, in shared memory): the last evaluation's
+// normalised features, class and margin (its logit minus the best other,
+// less a rounding allowance) are kept. With P the per-feature sensitivity
+// bound installed with the weights, no logit difference can have moved by
+// more than sum_i P[i] |f_i - f_last_i|; while that is below the margin the
+// network would pick the same class, so the layers are skipped. Long runs of
+// similar levels (a grid's ring of a few thousand vertices growing by a few
+// per level) then cost four shuffles instead of the network, and decisions
+// are those of evaluating the network at every level.
+__device__ int mlp_decide(const float* sw, const float* raw, int lane, float* cache_f, int* cache_dec,
+                          float* cache_margin) {
   const float* mean = sw;
   const float* sd = sw + 8;
   const float* W1T = sw + 16;
@@ -317,6 +323,7 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane, float* ca
   const float* B2 = W2T + 1024;
   const float* W3 = B2 + 32;
   const float* B3 = W3 + 96;
+  const float* P = B3 + 3;
   float f = 0.f;
   if (lane < 8) {
     const float r = raw[lane];
@@ -325,8 +332,14 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane, float* ca
     else f = log1pf(r > 0.f ? r : 0.f);
     f = (f - mean[lane]) / sd[lane];
   }
-  const bool near = lane >= 8 || fabsf(f - cache_f[lane]) < kMlpReuse;
-  if (__all_sync(0xffffffffu, near) && *cache_dec >= 0) return *cache_dec;
+  if (*cache_dec >= 0) {
+    float d = lane < 8 ? P[lane] * fabsf(f - cache_f[lane]) : 0.f;
+    d += __shfl_xor_sync(0xffffffffu, d, 4);
+    d += __shfl_xor_sync(0xffffffffu, d, 2);
+    d += __shfl_xor_sync(0xffffffffu, d, 1);
+    d = __shfl_sync(0xffffffffu, d, 0);  // sum over lanes 0..7
+    if (d < *cache_margin) return *cache_dec;
+  }
   float a = B1[lane];
 #pragma unroll
   for (int i = 0; i < 8; ++i) a = fmaf(W1T[i * 32 + lane], __shfl_sync(0xffffffffu, f, i), a);
@@ -342,9 +355,16 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane, float* ca
   int best = 0;
   if (o[1] > o[best]) best = 1;
   if (o[2] > o[best]) best = 2;
+  const int o1 = best == 0 ? 1 : 0, o2 = best == 2 ? 1 : 2;
+  const float second = fmaxf(o[o1], o[o2]);
+  // rounding allowance: the logits are float sums of a few dozen terms
+  const float slack = 1e-4f * (fabsf(o[best]) + fabsf(second) + 1.f);
   __syncwarp();
   if (lane < 8) cache_f[lane] = f;
-  if (lane == 0) *cache_dec = best;
+  if (lane == 0) {
+    *cache_dec = best;
+    *cache_margin = o[best] - second - slack;
+  }
   __syncwarp();
   return best;
 }
@@ -1309,7 +1329,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       // the learned switch: warp 0 evaluates it while the block waits (one
       // warp keeps the shared-memory and shuffle traffic of the network small)
       if (threadIdx.x < 32) {
-        int s2 = p.mlp ? mlp_decide(sm.mlp_w, sm.mlp_raw, threadIdx.x, sm.mlp_cache_f, &sm.mlp_cache_dec)
+        int s2 = p.mlp ? mlp_decide(sm.mlp_w, sm.mlp_raw, threadIdx.x, sm.mlp_cache_f, &sm.mlp_cache_dec,
+                                    &sm.mlp_cache_margin)
                        : XBFS_TD_QUEUE;
         if (s2 == XBFS_BU && !p.allow_bu) s2 = XBFS_TD_QUEUE;
         if (threadIdx.x == 0) sm.strategy = s2;

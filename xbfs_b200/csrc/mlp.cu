@@ -31,6 +31,7 @@ constexpr int kOffW3 = kOffB2 + kH;
 constexpr int kOffB3 = kOffW3 + kOut * kH;
 constexpr int kPacked = kOffB3 + kOut;  // 16 + 1443
 constexpr int kTrainable = kPacked - 16;
+constexpr int kMlpBound = 8;  // per-feature sensitivity bound stored after the installed weights
 
 static std::mutex g_mlp_mu;
 static float* g_mlp_dev[64] = {nullptr};
@@ -170,8 +171,39 @@ xbfs_status xbfs_mlp_set_weights(int32_t device, const float* packed, int32_t n)
     g_mlp_dev[device] = nullptr;
     return XBFS_OK;
   }
-  if (!g_mlp_dev[device]) XBFS_CUDA_TRY(cudaMalloc(&g_mlp_dev[device], kPacked * sizeof(float)));
-  XBFS_CUDA_TRY(cudaMemcpy(g_mlp_dev[device], packed, kPacked * sizeof(float), cudaMemcpyHostToDevice));
+  // The installed copy carries, after the packed weights, a per-feature
+  // sensitivity bound of the network (path bound through the ReLU layers):
+  //   P[i] = max over class pairs (a, b) of
+  //          sum_k |W3[a][k] - W3[b][k]| * sum_j |W2[k][j]| * |W1[j][i]|,
+  // so that moving the normalised features by d changes any logit
+  // difference by at most sum_i P[i] * |d_i|. The traversal kernel reuses
+  // its last decision while that bound stays below the decision's margin,
+  // i.e. only where evaluating the network again would give the same class.
+  std::vector<float> ext(kPacked + kMlpBound);
+  memcpy(ext.data(), packed, kPacked * sizeof(float));
+  const float* W1 = packed + kOffW1;
+  const float* W2 = packed + kOffW2;
+  const float* W3 = packed + kOffW3;
+  for (int i = 0; i < kIn; ++i) {
+    double h2[kH];  // sensitivity of each second-layer unit to feature i
+    for (int k = 0; k < kH; ++k) {
+      double t = 0;
+      for (int j = 0; j < kH; ++j) t += fabs((double)W2[k * kH + j]) * fabs((double)W1[j * kIn + i]);
+      h2[k] = t;
+    }
+    double worst = 0;
+    for (int a = 0; a < kOut; ++a)
+      for (int b = a + 1; b < kOut; ++b) {
+        double t = 0;
+        for (int k = 0; k < kH; ++k) t += fabs((double)W3[a * kH + k] - (double)W3[b * kH + k]) * h2[k];
+        worst = t > worst ? t : worst;
+      }
+    ext[kPacked + i] = (float)(worst * (1.0 + 1e-5));  // rounded up
+  }
+  if (!g_mlp_dev[device])
+    XBFS_CUDA_TRY(cudaMalloc(&g_mlp_dev[device], (kPacked + kMlpBound) * sizeof(float)));
+  XBFS_CUDA_TRY(cudaMemcpy(g_mlp_dev[device], ext.data(), (kPacked + kMlpBound) * sizeof(float),
+                           cudaMemcpyHostToDevice));
   return XBFS_OK;
 }
 
