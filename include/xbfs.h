@@ -298,6 +298,37 @@ xbfs_status xbfs_serve_release(xbfs_server* s, int32_t* levels_dev, int64_t V);
 xbfs_status xbfs_serve_fetch(xbfs_server* s, int32_t* levels_dev, int64_t V, int32_t* host_out);
 void xbfs_serve_free(xbfs_server* s);
 
+/* 1D-partitioned single-source BFS, the per-rank device steps (no reference
+ * counterpart: the reference runs one source on one GPU, cudaSetDevice at
+ * bfs_gpu_update.cu:138). Rank r owns the vertices [lo, hi) (lo a multiple
+ * of 32) and the CSR rows of those vertices (beg: hi - lo + 1 offsets into
+ * csr, which holds global neighbour ids). The host driver
+ * (xbfs_b200/partition.py) runs the level loop across ranks: a top-down
+ * level is xbfs_part_td_expand into a V-byte candidate array, a MAX
+ * all-reduce of that array, xbfs_part_claim; a bottom-up level (symmetric
+ * graphs) is xbfs_part_frontier_bits into this rank's words of a V-bit
+ * bitmap, an all-gather of the bitmap, xbfs_part_bottom_up. Candidate and
+ * bitmap buffers are device memory owned by the caller. Each call returns
+ * when its kernels have completed. */
+typedef struct xbfs_part xbfs_part;
+xbfs_status xbfs_part_create(const int64_t* beg, const int32_t* csr, int64_t V, int64_t lo, int64_t hi,
+                             int32_t symmetric, int32_t device, xbfs_part** out);
+void xbfs_part_free(xbfs_part* p);
+/* Levels -1, the source (if owned) level 0 and the only frontier vertex. */
+xbfs_status xbfs_part_reset(xbfs_part* p, int32_t src);
+/* out[4] = owned n_f, m_f (frontier vertices, their edges) and n_u, m_u
+ * (unvisited vertices with edges, their edges). */
+xbfs_status xbfs_part_stats(xbfs_part* p, int64_t* out);
+xbfs_status xbfs_part_td_expand(xbfs_part* p, uint8_t* cand);
+/* cand: after the all-reduce; cleared (all V bytes) on return. */
+xbfs_status xbfs_part_claim(xbfs_part* p, uint8_t* cand, int32_t next_level);
+/* slice: this rank's words of the global bitmap (nwords_slice >= ceil((hi-lo)/32)). */
+xbfs_status xbfs_part_frontier_bits(xbfs_part* p, uint32_t* slice, int64_t nwords_slice);
+/* fbits: the whole V-bit frontier bitmap after the all-gather. */
+xbfs_status xbfs_part_bottom_up(xbfs_part* p, const uint32_t* fbits, int32_t next_level);
+/* Levels of the owned vertices (hi - lo int32, host or device memory). */
+xbfs_status xbfs_part_levels(xbfs_part* p, int32_t* out);
+
 /* Per-level trace of the last xbfs_bfs call made with opts.trace = 1
  * (replaces the reference's tag[]/ratio[]/iter[] arrays, written to
  * Hybrid_iteration.csv at bfs_gpu_update.cu:270-272). */

@@ -158,6 +158,15 @@ SIGNATURES = {
     "xbfs_serve_release": (_i32, [_p, _p, _i64]),
     "xbfs_serve_fetch": (_i32, [_p, _p, _i64, _p]),
     "xbfs_serve_free": (None, [_p]),
+    "xbfs_part_create": (_i32, [_p, _p, _i64, _i64, _i64, _i32, _i32, C.POINTER(_p)]),
+    "xbfs_part_free": (None, [_p]),
+    "xbfs_part_reset": (_i32, [_p, _i32]),
+    "xbfs_part_stats": (_i32, [_p, _p]),
+    "xbfs_part_td_expand": (_i32, [_p, _p]),
+    "xbfs_part_claim": (_i32, [_p, _p, _i32]),
+    "xbfs_part_frontier_bits": (_i32, [_p, _p, _i64]),
+    "xbfs_part_bottom_up": (_i32, [_p, _p, _i32]),
+    "xbfs_part_levels": (_i32, [_p, _p]),
     "xbfs_mlp_num_params": (_i32, []),
     "xbfs_mlp_set_weights": (_i32, [_i32, _p, _i32]),
     "xbfs_mlp_logits": (_i32, [_i32, _p, _p, _i32, _p]),
