@@ -88,9 +88,14 @@ typedef struct xbfs_opts {
                            reference is wrong for padding > 1) */
   float beamer_alpha;   /* XBFS_POLICY_BEAMER: TD->BU when m_f > m_u/alpha (14) */
   float beamer_beta;    /*                     BU->TD when n_f < V/beta (24)   */
-  int32_t bu_probe;     /* bottom-up neighbour loads: 0 = 2, 4, then 8 at a time
-                           through L1 (default); 1 = the same, streaming (L1
-                           bypass); 2 = 4 at a time, streaming */
+  int32_t bu_probe;     /* bottom-up probe shape: 0 = word-parallel, each lane
+                           probing the first 4 neighbours of two vertices at
+                           once, longer scans deferred to a per-CTA queue
+                           (default); over a list of unvisited vertices:
+                           1 = 2, 4, then 8 neighbours at a time, streaming
+                           (L1 bypass); 2 = 4 at a time, streaming; 3 = two
+                           vertices per lane; 4 = 2, 4, then 8 at a time
+                           through L1 */
   int32_t wait_timeout_us; /* bound of every device-side wait of a traversal
                               (grid barriers); 0 = 10 s. On expiry the call
                               returns XBFS_ERR_DEVICE_TIMEOUT */

@@ -204,9 +204,10 @@ struct __align__(16) Smem {
   long long red[kBlock / 32 + 1];
   long long red4[4 * (kBlock / 32)];
   float mlp_raw[8];             // statistics the learned switch's features come from
-  float mlp_cache_f[8];         // features of its last evaluation
+  float mlp_cache_raw[8];       // statistics of its last evaluation
   int mlp_cache_dec;            // and its decision (-1: none yet)
   float mlp_cache_margin;       // and that decision's margin
+  float mlp_q[8];               // sensitivity bound per feature over the feature's scale
   LoopState ls;
   float mlp_w[1472];            // the learned switch's weights and bound (XBFS_POLICY_MLP); must stay last
 };
@@ -304,16 +305,18 @@ __device__ void mlp_stage(const float* __restrict__ w, float* sw) {
 // strategy; log growth of the frontier; log1p of its mean degree), one per
 // lane, then the three layers with the hidden activations passed by shuffles.
 // Called by one full warp.
-// Certified reuse (per CTA, in shared memory): the last evaluation's
-// normalised features, class and margin (its logit minus the best other,
+// Certified reuse (mlp_reuse_bound, per CTA, in shared memory): the last
+// evaluation's statistics, class and margin (its logit minus the best other,
 // less a rounding allowance) are kept. With P the per-feature sensitivity
 // bound installed with the weights, no logit difference can have moved by
-// more than sum_i P[i] |f_i - f_last_i|; while that is below the margin the
-// network would pick the same class, so the layers are skipped. Long runs of
-// similar levels (a grid's ring of a few thousand vertices growing by a few
-// per level) then cost four shuffles instead of the network, and decisions
-// are those of evaluating the network at every level.
-__device__ int mlp_decide(const float* sw, const float* raw, int lane, float* cache_f, int* cache_dec,
+// more than sum_i P[i] |x_i - x_last_i| over the normalised features x;
+// while a bound of that sum computed from the raw statistics stays below the
+// margin the network would pick the same class, and thread 0 reuses it
+// without running the layers or a second block barrier. Long runs of similar
+// levels (a grid's ring of a few thousand vertices growing by a few per
+// level) then cost a few scalar operations, and decisions are those of
+// evaluating the network at every level.
+__device__ int mlp_decide(const float* sw, const float* raw, int lane, float* cache_raw, int* cache_dec,
                           float* cache_margin) {
   const float* mean = sw;
   const float* sd = sw + 8;
@@ -332,14 +335,7 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane, float* ca
     else f = log1pf(r > 0.f ? r : 0.f);
     f = (f - mean[lane]) / sd[lane];
   }
-  if (*cache_dec >= 0) {
-    float d = lane < 8 ? P[lane] * fabsf(f - cache_f[lane]) : 0.f;
-    d += __shfl_xor_sync(0xffffffffu, d, 4);
-    d += __shfl_xor_sync(0xffffffffu, d, 2);
-    d += __shfl_xor_sync(0xffffffffu, d, 1);
-    d = __shfl_sync(0xffffffffu, d, 0);  // sum over lanes 0..7
-    if (d < *cache_margin) return *cache_dec;
-  }
+  (void)P;
   float a = B1[lane];
 #pragma unroll
   for (int i = 0; i < 8; ++i) a = fmaf(W1T[i * 32 + lane], __shfl_sync(0xffffffffu, f, i), a);
@@ -360,7 +356,7 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane, float* ca
   // rounding allowance: the logits are float sums of a few dozen terms
   const float slack = 1e-4f * (fabsf(o[best]) + fabsf(second) + 1.f);
   __syncwarp();
-  if (lane < 8) cache_f[lane] = f;
+  if (lane < 8) cache_raw[lane] = raw[lane];
   if (lane == 0) {
     *cache_dec = best;
     *cache_margin = o[best] - second - slack;
@@ -369,6 +365,24 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane, float* ca
   return best;
 }
 
+
+// Upper bound (with a rounding allowance) of sum_i P[i] |x_i - x_last_i| from
+// the raw statistics a (now) and b (last evaluation), q[i] = P[i] / scale_i:
+// |log1p(u) - log1p(v)| <= |u - v| / (1 + min(u, v)) for the log features;
+// the growth feature log1p(n_f) - log1p(n_prev) moves by at most the sum of
+// its two terms' moves; the previous strategy enters as it is.
+__device__ __forceinline__ float mlp_dlog1p(float u, float v) {
+  u = fmaxf(u, 0.f);
+  v = fmaxf(v, 0.f);
+  return fabsf(u - v) / (1.f + fminf(u, v));
+}
+__device__ float mlp_reuse_bound(const float* a, const float* b, const float* q) {
+  const float d0 = mlp_dlog1p(a[0], b[0]);
+  float t = q[0] * d0 + q[1] * mlp_dlog1p(a[1], b[1]) + q[2] * mlp_dlog1p(a[2], b[2]) +
+            q[3] * mlp_dlog1p(a[3], b[3]) + q[4] * mlp_dlog1p(a[4], b[4]) + q[5] * fabsf(a[5] - b[5]) +
+            q[6] * (d0 + mlp_dlog1p(a[6], b[6])) + q[7] * mlp_dlog1p(a[7], b[7]);
+  return t * 1.001f + 1e-6f;
+}
 
 // ---------------------------------------------------------------------------
 // Staging of top-down winners (per CTA) and flush to the global binned queue.
@@ -1086,6 +1100,158 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
   }
 }
 
+// Bottom-up step for level L, word-parallel (the default probe mode). Each
+// warp takes kBuWords consecutive words of its CTA's slice of the visited
+// bitmap at a time; lane i handles vertex 32w+i of each word when it is
+// unvisited. A lane's vertices are probed together: their CSR offsets, then
+// the first kBuFirst neighbours of each, then those neighbours' frontier
+// bits, so every lane keeps kBuWords x kBuFirst loads in flight and a warp
+// crosses its slice in few dependent steps. No list of unvisited vertices
+// is built (the bitmap word is the lanes' work), and results go out with
+// one atomic per word. On power-law graphs most unvisited vertices find a
+// parent within the first few neighbours; one that still has neighbours
+// left is deferred to a per-CTA queue in shared memory (the top-down staging
+// areas, unused in a bottom-up level) and drained afterwards one vertex per
+// lane, kBuMore neighbours per step, so a long scan no longer holds the 31
+// other lanes of its warp.
+constexpr int kBuWords = 2, kBuFirst = 4, kBuMore = 8;
+constexpr int kBuQueue = 2 * kCap;
+
+template <bool PAR, bool ASYNC>
+__device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
+                                uint32_t* fbn2) {
+  const long long nw = p.nwords;
+  const long long G = gridDim.x, b = blockIdx.x;
+  const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NWARP = kBlock / 32;
+  int* q_v = &sm.st_id[0][0];        // deferred vertex
+  long long* q_e = &sm.st_bg[0][0];  // its next neighbour to probe
+  if (threadIdx.x == 0) {
+    sm.bu_n = 0;
+    sm.bu_next = 0;
+  }
+  __syncthreads();
+  for (long long wb = w0 + (long long)warp * kBuWords; wb < w1; wb += (long long)NWARP * kBuWords) {
+    uint32_t un[kBuWords];
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k) un[k] = (wb + k < w1) ? ~ld_cg_u32(p.vis + wb + k) : 0u;
+    long long e[kBuWords], ee[kBuWords];
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k) {
+      e[k] = 0;
+      ee[k] = 0;
+      if ((un[k] >> lane) & 1u) {
+        const int v = (int)((wb + k) * 32 + lane);
+        e[k] = ld_nc_i64(p.beg + v);
+        ee[k] = ld_nc_i64(p.beg + v + 1);
+      }
+    }
+    int u[kBuWords][kBuFirst];
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k)
+#pragma unroll
+      for (int j = 0; j < kBuFirst; ++j) u[k][j] = (e[k] + j < ee[k]) ? __ldg(p.csr + e[k] + j) : -1;
+    uint32_t wc[kBuWords][kBuFirst];
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k)
+#pragma unroll
+      for (int j = 0; j < kBuFirst; ++j) wc[k][j] = (u[k][j] >= 0) ? fbc[u[k][j] >> 5] : 0u;
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k) {
+      const bool act = (un[k] >> lane) & 1u;
+      int found = -1, found2 = -1;
+#pragma unroll
+      for (int j = 0; j < kBuFirst; ++j)
+        if (found < 0 && u[k][j] >= 0 && ((wc[k][j] >> (u[k][j] & 31)) & 1u)) found = u[k][j];
+      const long long d = ee[k] - e[k];
+      bool defer = act && found < 0 && d > kBuFirst;
+      // warp-aggregated slots in the deferred queue; a full queue is not an
+      // error: the lane then scans the rest of its vertex here
+      const unsigned dm = __ballot_sync(0xffffffffu, defer);
+      if (dm) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&sm.bu_n, __popc(dm));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (defer) {
+          const int slot = base + __popc(dm & ((1u << lane) - 1u));
+          if (slot < kBuQueue) {
+            q_v[slot] = (int)((wb + k) * 32 + lane);
+            q_e[slot] = e[k] + kBuFirst;
+          } else {
+            long long ex = e[k] + kBuFirst;
+            probe_range<kBuMore, true, ASYNC>(p, fbc, fbn, ex, ee[k], found, found2);
+            defer = false;
+          }
+        }
+      }
+      if (ASYNC && act && found < 0 && !defer && found2 < 0) {
+        // whole neighbour list scanned without a level-L parent: a neighbour
+        // already in frontier L+1 gives level L+2
+#pragma unroll
+        for (int j = 0; j < kBuFirst; ++j)
+          if (found2 < 0 && u[k][j] >= 0 && ((ld_cg_u32(fbn + (u[k][j] >> 5)) >> (u[k][j] & 31)) & 1u))
+            found2 = u[k][j];
+      }
+      const bool got1 = act && found >= 0;
+      const bool got2 = ASYNC && act && !got1 && !defer && found2 >= 0;
+      const int v = (int)((wb + k) * 32 + lane);
+      if (got1) {
+        p.levels[v] = L + 1;
+        if (PAR) p.parents[v] = found;
+        acc.n1 += 1;
+        acc.m1 += d;
+      } else if (got2) {
+        p.levels[v] = L + 2;
+        if (PAR) p.parents[v] = found2;
+        acc.n2 += 1;
+        acc.m2 += d;
+      }
+      const uint32_t m1 = __ballot_sync(0xffffffffu, got1);
+      const uint32_t m2 = __ballot_sync(0xffffffffu, got2);
+      if (lane == 0 && (m1 | m2)) {
+        const long long w = wb + k;
+        red_or_u32(p.vis + w, m1 | m2);
+        if (m1) red_or_u32(fbn + w, m1);
+        if (ASYNC && m2) red_or_u32(fbn2 + w, m2);
+      }
+    }
+  }
+  __syncthreads();
+  const int nq = sm.bu_n < kBuQueue ? sm.bu_n : kBuQueue;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&sm.bu_next, 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= nq) break;
+    const int i = base + lane;
+    uint32_t word = 0xffffffffu, m1 = 0, m2 = 0;
+    if (i < nq) {
+      const int v = q_v[i];
+      long long e = q_e[i];
+      const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
+      int found = -1, found2 = -1;
+      probe_range<kBuMore, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+      word = (uint32_t)v >> 5;
+      const uint32_t bit = 1u << (v & 31);
+      if (found >= 0) {
+        p.levels[v] = L + 1;
+        if (PAR) p.parents[v] = found;
+        m1 = bit;
+        acc.n1 += 1;
+        acc.m1 += e1 - e0;
+      } else if (ASYNC && found2 >= 0) {
+        p.levels[v] = L + 2;
+        if (PAR) p.parents[v] = found2;
+        m2 = bit;
+        acc.n2 += 1;
+        acc.m2 += e1 - e0;
+      }
+    }
+    bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, m2, i < nq);
+  }
+}
+
 // Block-reduce the accumulators and publish them to the frontier descriptors.
 __device__ void publish_acc(Smem& sm, Acc& acc, FDesc* f1, FDesc* f2) {
   long long v[4] = {acc.n1, acc.m1, acc.n2, acc.m2};
@@ -1190,6 +1356,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
   // inner loop of the level.
   LoopState& ls = sm.ls;
   if (threadIdx.x == 0) {
+    if (p.policy == XBFS_POLICY_MLP && p.mlp) {
+      // the installed bound after the weights, over each feature's scale
+      const float* sd = sm.mlp_w + 8;
+      const float* P = sm.mlp_w + kMlpParams;
+      for (int k = 0; k < 8; ++k) sm.mlp_q[k] = P[k] / sd[k];
+    }
     ls.ps.count_prev = 0;
     ls.ps.is_change = 0;
     ls.ps.td_adaptive = kInfinite;
@@ -1292,24 +1464,23 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
           case XBFS_POLICY_BEAMER:
             s = decide_beamer(ls.ps, n_f, m_f, m_u, p.V, p.beamer_alpha, p.beamer_beta);
             break;
-          case XBFS_POLICY_MLP:
-            s = -2;  // decided by warp 0 below
+          case XBFS_POLICY_MLP: {
+            const float raw[8] = {(float)n_f, (float)m_f, (float)n_u, (float)m_u, (float)L,
+                                  (float)ls.ps.prev_strategy, (float)ls.ps.n_prev,
+                                  (float)((double)m_f / (double)n_f)};
+            if (sm.mlp_cache_dec >= 0 && mlp_reuse_bound(raw, sm.mlp_cache_raw, sm.mlp_q) < sm.mlp_cache_margin) {
+              s = sm.mlp_cache_dec;  // certified: the network would choose the same
+            } else {
+              s = -2;  // decided by warp 0 below
+#pragma unroll
+              for (int k = 0; k < 8; ++k) sm.mlp_raw[k] = raw[k];
+            }
             break;
+          }
           default:
             s = decide_reference(ls.ps, L, m_f, p.E, p.alpha);
         }
         if (s == XBFS_BU && !p.allow_bu) s = XBFS_TD_QUEUE;
-        if (s == -2) {
-          // raw statistics; every warp forms the features and runs the network
-          sm.mlp_raw[0] = (float)n_f;
-          sm.mlp_raw[1] = (float)m_f;
-          sm.mlp_raw[2] = (float)n_u;
-          sm.mlp_raw[3] = (float)m_u;
-          sm.mlp_raw[4] = (float)L;
-          sm.mlp_raw[5] = (float)ls.ps.prev_strategy;
-          sm.mlp_raw[6] = (float)ls.ps.n_prev;
-          sm.mlp_raw[7] = (float)((double)m_f / (double)n_f);
-        }
         if (blockIdx.x == 0 && L < p.hist_cap) {
           LevelRecDev& r = p.hist[L];
           r.n_f = n_f;
@@ -1329,7 +1500,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       // the learned switch: warp 0 evaluates it while the block waits (one
       // warp keeps the shared-memory and shuffle traffic of the network small)
       if (threadIdx.x < 32) {
-        int s2 = p.mlp ? mlp_decide(sm.mlp_w, sm.mlp_raw, threadIdx.x, sm.mlp_cache_f, &sm.mlp_cache_dec,
+        int s2 = p.mlp ? mlp_decide(sm.mlp_w, sm.mlp_raw, threadIdx.x, sm.mlp_cache_raw, &sm.mlp_cache_dec,
                                     &sm.mlp_cache_margin)
                        : XBFS_TD_QUEUE;
         if (s2 == XBFS_BU && !p.allow_bu) s2 = XBFS_TD_QUEUE;
@@ -1409,10 +1580,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         dirty |= 1u << (L & 3);
         if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       }
-      if (p.async_bu)
+      if (p.bu_mode == 0) {
+        if (p.async_bu)
+          bottom_up_words<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+        else
+          bottom_up_words<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+      } else if (p.async_bu) {
         bottom_up<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
-      else
+      } else {
         bottom_up<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+      }
       publish_acc(sm, acc, F1, F2);
       if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       q_valid = false;

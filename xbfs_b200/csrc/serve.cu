@@ -340,7 +340,17 @@ __device__ void sv_tick_bu(const Params& p, long long t, unsigned long long bu, 
       if (needed) {
         const long long b0 = ld_nc_i64(p.beg + v), b1 = ld_nc_i64(p.beg + v + 1);
         unsigned long long got = 0;
-        for (long long e = b0; e < b1 && got != needed; ++e) got |= ld_cg_u64(Fc + ld_stream_i32(p.csr + e)) & needed;
+        // four neighbours per step: their CSR entries, then their masks, are
+        // loaded together, so a lane has four probes in flight
+        for (long long e = b0; e < b1 && got != needed; e += 4) {
+          int u[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) u[k] = (e + k < b1) ? ld_stream_i32(p.csr + e + k) : -1;
+          unsigned long long f[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) f[k] = (u[k] >= 0) ? ld_cg_u64(Fc + u[k]) : 0ull;
+          got |= (f[0] | f[1] | f[2] | f[3]) & needed;
+        }
         if (got) {
           deg = b1 - b0;
           vb0 = b0;
