@@ -88,10 +88,12 @@ typedef struct xbfs_opts {
                            reference is wrong for padding > 1) */
   float beamer_alpha;   /* XBFS_POLICY_BEAMER: TD->BU when m_f > m_u/alpha (14) */
   float beamer_beta;    /*                     BU->TD when n_f < V/beta (24)   */
-  int32_t bu_probe;     /* bottom-up probe shape: 0 = word-parallel, each lane
-                           probing the first 4 neighbours of two vertices at
-                           once, longer scans deferred to a per-CTA queue
-                           (default); over a list of unvisited vertices:
+  int32_t bu_probe;     /* bottom-up probe shape: 0 = by density (default):
+                           while unvisited vertices are at least V/4,
+                           word-parallel (5), else over a compacted list of
+                           them (4); 5 = word-parallel, each lane probing the
+                           first 4 neighbours of two vertices at once, longer
+                           scans deferred to a per-CTA queue; over the list:
                            1 = 2, 4, then 8 neighbours at a time, streaming
                            (L1 bypass); 2 = 4 at a time, streaming; 3 = two
                            vertices per lane; 4 = 2, 4, then 8 at a time

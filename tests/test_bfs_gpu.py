@@ -224,7 +224,7 @@ def test_many_sources_pipelined_equal_single_calls(out, kind):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("bu_mode", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("bu_mode", [0, 1, 2, 3, 4, 5])
 def test_bottom_up_probe_modes(bu_mode):
     """Every bottom-up probe shape gives the oracle's levels and a valid tree
     (R-MAT with async bottom-up on and off, and a forced all-bottom-up run)."""

@@ -197,6 +197,7 @@ struct __align__(16) Smem {
   int next_s;
   int bu_next;
   int bu_n;
+  int bu_dense;                 // this level's unvisited vertices are at least a quarter of V
   int chunk;
   unsigned long long bins[3];   // F_L bin counters, read once per level
   long long pend_next;          // F_{L+1} entries already found (async bottom-up)
@@ -374,14 +375,14 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane, float* ca
 __device__ __forceinline__ float mlp_dlog1p(float u, float v) {
   u = fmaxf(u, 0.f);
   v = fmaxf(v, 0.f);
-  return fabsf(u - v) / (1.f + fminf(u, v));
+  return __fdividef(fabsf(u - v), 1.f + fminf(u, v));  // approximate: the sum's allowance below covers it
 }
 __device__ float mlp_reuse_bound(const float* a, const float* b, const float* q) {
   const float d0 = mlp_dlog1p(a[0], b[0]);
   float t = q[0] * d0 + q[1] * mlp_dlog1p(a[1], b[1]) + q[2] * mlp_dlog1p(a[2], b[2]) +
             q[3] * mlp_dlog1p(a[3], b[3]) + q[4] * mlp_dlog1p(a[4], b[4]) + q[5] * fabsf(a[5] - b[5]) +
             q[6] * (d0 + mlp_dlog1p(a[6], b[6])) + q[7] * mlp_dlog1p(a[7], b[7]);
-  return t * 1.001f + 1e-6f;
+  return t * 1.01f + 1e-6f;
 }
 
 // ---------------------------------------------------------------------------
@@ -821,18 +822,46 @@ __device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc
     }
     __syncthreads();
     // 3. edge-balanced expansion of the tile
-    for (long long r = 0; r < T; r += kTE) {
+    if (!enq) {
+      // bitmap output: nothing is staged, so the rounds need no block
+      // barrier; each thread keeps four edges in flight (their neighbour
+      // ids, then the visited words of all four) and claims only the
+      // targets that looked unvisited
+      for (long long e0 = threadIdx.x; e0 < T; e0 += 4 * kBlock) {
+        int v[4], u[4];
 #pragma unroll
-      for (int k = 0; k < kK; ++k) {
-        const long long e = r + threadIdx.x + (long long)k * kBlock;
-        if (e < T) {
-          const int a = smem_owner(sm.web, n, (unsigned long long)e);
-          const int v = __ldg(p.csr + sm.wbeg[a] + (e - (long long)sm.web[a]));
-          claim_td<PAR>(p, sm, q, acc, v, sm.wu[a], L, enq, fbn, spec);
+        for (int k = 0; k < 4; ++k) {
+          const long long e = e0 + (long long)k * kBlock;
+          v[k] = -1;
+          u[k] = 0;
+          if (e < T) {
+            const int a = smem_owner(sm.web, n, (unsigned long long)e);
+            v[k] = __ldg(p.csr + sm.wbeg[a] + (e - (long long)sm.web[a]));
+            u[k] = sm.wu[a];
+          }
         }
+        uint32_t vw[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (v[k] >= 0 && !((vw[k] >> (v[k] & 31)) & 1u)) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, false, fbn, true);
       }
-      __syncthreads();
-      if (enq && need_flush(sm)) flush(sm, q);
+      __syncthreads();  // the next chunk rewrites the window
+    } else {
+      for (long long r = 0; r < T; r += kTE) {
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+          const long long e = r + threadIdx.x + (long long)k * kBlock;
+          if (e < T) {
+            const int a = smem_owner(sm.web, n, (unsigned long long)e);
+            const int v = __ldg(p.csr + sm.wbeg[a] + (e - (long long)sm.web[a]));
+            claim_td<PAR>(p, sm, q, acc, v, sm.wu[a], L, enq, fbn, spec);
+          }
+        }
+        __syncthreads();
+        if (need_flush(sm)) flush(sm, q);
+      }
     }
   }
   }
@@ -1454,6 +1483,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         long long m_u = p.E - ls.vis_m - pm;
         if (n_u < 0) n_u = 0;
         if (m_u < 0) m_u = 0;
+        sm.bu_dense = (n_u * 4 >= p.V) ? 1 : 0;
         switch (p.policy) {
           case XBFS_POLICY_FORCED: {
             const long long i = L < p.n_forced ? L : p.n_forced - 1;
@@ -1466,8 +1496,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
             break;
           case XBFS_POLICY_MLP: {
             const float raw[8] = {(float)n_f, (float)m_f, (float)n_u, (float)m_u, (float)L,
-                                  (float)ls.ps.prev_strategy, (float)ls.ps.n_prev,
-                                  (float)((double)m_f / (double)n_f)};
+                                  (float)ls.ps.prev_strategy, (float)ls.ps.n_prev, (float)m_f / (float)n_f};
             if (sm.mlp_cache_dec >= 0 && mlp_reuse_bound(raw, sm.mlp_cache_raw, sm.mlp_q) < sm.mlp_cache_margin) {
               s = sm.mlp_cache_dec;  // certified: the network would choose the same
             } else {
@@ -1580,7 +1609,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         dirty |= 1u << (L & 3);
         if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       }
-      if (p.bu_mode == 0) {
+      // word-parallel while unvisited vertices are dense (the first
+      // bottom-up level of a power-law graph), else over the compacted list
+      // of unvisited vertices (few per bitmap word: most lanes of a word
+      // would idle)
+      if (p.bu_mode == 5 || (p.bu_mode == 0 && sm.bu_dense)) {
         if (p.async_bu)
           bottom_up_words<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
         else

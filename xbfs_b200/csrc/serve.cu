@@ -702,6 +702,12 @@ static xbfs_status engine_step(Server* srv, bool oom_is_error, bool* active, boo
       }
     }
     b.tick += k;
+    // a request still running after t ticks is at least t levels deep: a
+    // graph whose traversals are long is known as such before any finishes
+    for (unsigned long long m = b.busy & ~finished; m; m &= m - 1) {
+      const ServeRequest& r = srv->reqs[b.req_of_slot[__builtin_ctzll(m)]];
+      b.depth_est = std::max(b.depth_est, (int)std::min<long long>(b.tick - r.join, 1 << 30));
+    }
     if (!finished) {
       // longer rounds while nothing finishes, but never beyond an eighth of
       // the depth seen on this graph (a low-diameter graph keeps short rounds,
@@ -931,6 +937,23 @@ xbfs_status xbfs_serve_create(xbfs_graph* const* graphs, int32_t n, int32_t devi
   uint64_t thr = UINT64_MAX;
   XBFS_CUDA_TRY(cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &thr));
   XBFS_CUDA_TRY(cudaStreamCreateWithFlags(&srv->release_stream, cudaStreamNonBlocking));
+  // grow the pool once to room for 16 level arrays of the largest graph (at
+  // most half the budget), so the first requests of a run do not pay for
+  // the pool's growth; the release threshold keeps the memory in the pool
+  {
+    size_t vmax = 0;
+    for (auto& b : srv->batches) vmax = std::max(vmax, (size_t)b->g->V * 4);
+    const size_t warm = std::min(vmax * 16, srv->budget / 2);
+    if (warm > 0) {
+      void* mem = nullptr;
+      cudaStream_t s0 = srv->batches[0]->stream;
+      if (cudaMallocFromPoolAsync(&mem, warm, srv->pool, s0) == cudaSuccess) {
+        XBFS_CUDA_TRY(cudaFreeAsync(mem, s0));
+      } else {
+        cudaGetLastError();  // not enough memory for the warm-up: the pool grows on demand instead
+      }
+    }
+  }
   XBFS_CUDA_TRY(cudaDeviceSynchronize());
   *out = (xbfs_server*)srv.release();
   return XBFS_OK;
