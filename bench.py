@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--sources", type=int, default=64)
     ap.add_argument("--policy", default="heuristic")
+    ap.add_argument("--adjacency", choices=["degree", "file"], default="degree",
+                    help="neighbour order prepared before timing: descending neighbour degree (default) or as "
+                         "generated (ascending ids); levels are the same either way")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-flush", action="store_true")
@@ -268,6 +271,10 @@ def run_ours(args):
     dev = local
     g, wname = make_graph(args, dev)
     V, E = g.V, g.E
+    if args.adjacency == "degree":
+        # graph preparation, untimed: hubs first in every neighbour list, so
+        # bottom-up probes find a frontier parent sooner (levels unchanged)
+        g.sort_adjacency("degree")
     beg = g.offsets()
     srcs = pick_sources(beg, args.sources, args.seed + rank)
     # a dedicated stream: the library launches on it, and the events, the L2
@@ -322,6 +329,22 @@ def run_ours(args):
     n_par = 0 if args.no_parity else min(16, len(plan[-1]))
     par_src = [int(x) for x in plan[-1][:n_par]]
     par_rows = rows[:n_par].cpu().numpy() if n_par else None
+    # the same timed path on the neighbour order as generated, for reference
+    file_order = None
+    if args.adjacency == "degree":
+        g.sort_adjacency("id")
+        g.bfs_many(plan[0][:2], levels=rows[:2], opts=opts)
+        fe0, fe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fedges = 0
+        fe0.record(stream)
+        for src_chunk in plan:
+            fedges += g.bfs_many(src_chunk, levels=rows[:len(src_chunk)], opts=opts).edges_mc
+        fe1.record(stream)
+        torch.cuda.synchronize()
+        fms = fe0.elapsed_time(fe1)
+        file_order = {"gteps": round(fedges / (fms * 1e-3) / 1e9, 3), "ms_per_step": round(fms / args.steps, 5),
+                      "note": "same sources and timed path, neighbours in generator order"}
+        g.sort_adjacency("degree")
     del rows
 
     # ---- one xbfs_bfs call per step with the L2 flushed before each (the
@@ -410,6 +433,7 @@ def run_ours(args):
         "timed_region": "xbfs_bfs_many over the steps' sources, level rows in HBM; the per-call figures flush "
                         "L2 (256 MB write + 256 MB read, untimed) before each call",
         "median_depth": depth, "levels_by_strategy": strat, "parity": parity,
+        "adjacency_generator_order": file_order,
         "per_call_l2_flushed": {"gteps": round(pc_gteps, 3), "steps": pc_steps,
                                 "ms_per_step": round(sum(step_ms) / pc_steps, 5),
                                 "kernel_ms_mean": round(statistics.mean(kernel_ms), 5)},
@@ -663,8 +687,10 @@ def workload_config(args, V, E, n_sources, world):
         wname = f"rmat-s{args.scale}-ef{args.ef}"
     else:
         wname = f"grid-{args.grid_w}x{args.grid_h}"
+    adjacency = ("neighbours of each vertex in descending degree order (untimed preparation)"
+                 if args.adjacency == "degree" else "neighbours in generator order (ascending ids)")
     return {"workload": f"{wname} single-source BFS", "V": int(V), "E": int(E), "sources": int(n_sources),
-            "policy": args.policy, "seed": args.seed,
+            "policy": args.policy, "seed": args.seed, "adjacency": adjacency,
             "l2": "inputs larger than L2 (CSR of E int32 entries) in the timed steps",
             "parallelism": f"replicas x{world}"}
 
@@ -741,6 +767,8 @@ def run_reference(args):
     else:
         beg, csr = oracle.gen_grid(args.grid_w, args.grid_h)
     srcs = oracle.pick_sources(beg, args.sources, args.seed)
+    if args.adjacency == "degree":
+        csr = oracle.sort_adjacency_degree(beg, csr)   # the same graph preparation as the other arm
     for i in range(args.warmup):
         oracle.bfs_sweep(beg, csr, srcs[i % len(srcs)], threads)
     t_total, edges = 0.0, 0

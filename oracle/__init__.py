@@ -64,6 +64,8 @@ def _load():
     lib.oracle_gen_grid.argtypes = [C.c_int32, C.c_int32, pp, pp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.oracle_pick_sources.restype = C.c_int32
     lib.oracle_pick_sources.argtypes = [p, C.c_int64, C.c_int32, C.c_uint64, p]
+    lib.oracle_sort_adjacency_degree.restype = C.c_int32
+    lib.oracle_sort_adjacency_degree.argtypes = [p, p, C.c_int64]
     lib.oracle_free.restype = None
     lib.oracle_free.argtypes = [C.c_void_p]
     return lib
@@ -201,3 +203,13 @@ def pick_sources(beg, k: int, seed: int = 1) -> np.ndarray:
     if _lib.oracle_pick_sources(beg.ctypes.data, len(beg) - 1, k, seed, out.ctypes.data) != 0:
         raise ValueError("graph has no edges")
     return out[:k]
+
+
+def sort_adjacency_degree(beg, csr) -> np.ndarray:
+    """The CSR's neighbour lists reordered by descending neighbour degree
+    (ties by ascending id); returns a new csr array."""
+    beg = np.ascontiguousarray(beg, dtype=np.int64)
+    out = np.array(csr, dtype=np.int32, copy=True)
+    if _lib.oracle_sort_adjacency_degree(beg.ctypes.data, out.ctypes.data, len(beg) - 1) != 0:
+        raise MemoryError("oracle_sort_adjacency_degree failed")
+    return out

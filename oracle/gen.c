@@ -264,3 +264,40 @@ int32_t oracle_pick_sources(const int64_t* beg, int64_t V, int32_t k, uint64_t s
   }
   return 0;
 }
+
+static int ogen_cmp_u64(const void* a, const void* b) {
+  const uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+  return (x > y) - (x < y);
+}
+
+/* Reorders each vertex's neighbours by descending neighbour degree, ties by
+ * ascending id (the order the library's xbfs_graph_sort_adjacency gives an
+ * id-sorted CSR). In place; returns 0, or -2 when out of memory. */
+int32_t oracle_sort_adjacency_degree(const int64_t* beg, int32_t* csr, int64_t V) {
+  int64_t maxd = 0;
+  for (int64_t v = 0; v < V; ++v) maxd = beg[v + 1] - beg[v] > maxd ? beg[v + 1] - beg[v] : maxd;
+  int failed = 0;
+#pragma omp parallel
+  {
+    uint64_t* key = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(maxd > 0 ? maxd : 1));
+    if (!key) {
+#pragma omp atomic write
+      failed = 1;
+    }
+#pragma omp for schedule(dynamic, 1024)
+    for (int64_t v = 0; v < V; ++v) {
+      if (!key) continue;
+      const int64_t b = beg[v], n = beg[v + 1] - b;
+      if (n < 2) continue;
+      for (int64_t i = 0; i < n; ++i) {
+        const int32_t u = csr[b + i];
+        const uint64_t d = (uint64_t)(beg[u + 1] - beg[u]);
+        key[i] = ((uint64_t)(uint32_t)~(uint32_t)(d > 0xffffffffull ? 0xffffffffull : d) << 32) | (uint32_t)u;
+      }
+      qsort(key, (size_t)n, sizeof(uint64_t), ogen_cmp_u64);
+      for (int64_t i = 0; i < n; ++i) csr[b + i] = (int32_t)(key[i] & 0xffffffffull);
+    }
+    free(key);
+  }
+  return failed ? -2 : 0;
+}

@@ -78,7 +78,7 @@ def test_reference_arm_under_torchrun_prints_once():
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] in ("port", "reference") and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["config"]["workload"] == "rmat-s12-ef8 single-source BFS" and d["config"]["sources"] == 4
-    assert set(d["config"]) == {"workload", "V", "E", "sources", "policy", "seed", "l2", "parallelism"}
+    assert set(d["config"]) == {"workload", "V", "E", "sources", "policy", "seed", "adjacency", "l2", "parallelism"}
     assert "reference_gpu" in d
 
 

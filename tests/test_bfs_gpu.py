@@ -254,6 +254,8 @@ def test_degree_sorted_adjacency_keeps_levels():
         seg, seg2 = csr[beg[u]:beg[u + 1]], c2[beg[u]:beg[u + 1]]
         assert np.array_equal(np.sort(seg), np.sort(seg2))
         assert np.all(np.diff(deg[seg2]) <= 0)
+    # the same order as the oracle side builds for the reference arm (ties by id)
+    assert np.array_equal(c2, oracle.sort_adjacency_degree(beg, csr))
     for s in pick_sources(beg, 4, 3):
         r = g.bfs(int(s), want_parents=True)
         assert np.array_equal(r.levels, oracle.bfs_queue(beg, csr, int(s)))

@@ -1143,7 +1143,13 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
 // areas, unused in a bottom-up level) and drained afterwards one vertex per
 // lane, kBuMore neighbours per step, so a long scan no longer holds the 31
 // other lanes of its warp.
-constexpr int kBuWords = 2, kBuFirst = 4, kBuMore = 8;
+#ifndef XBFS_BU_WORDS
+#define XBFS_BU_WORDS 2
+#endif
+#ifndef XBFS_BU_FIRST
+#define XBFS_BU_FIRST 4
+#endif
+constexpr int kBuWords = XBFS_BU_WORDS, kBuFirst = XBFS_BU_FIRST, kBuMore = 8;
 constexpr int kBuQueue = 2 * kCap;
 
 template <bool PAR, bool ASYNC>
