@@ -100,3 +100,25 @@ def test_decisions_are_the_networks_at_every_level(kind):
         assert checked > 0
     finally:
         learned.install(None)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(os.path.dirname(__file__)), "xbfs_b200",
+                                                    "switch_mlp.npz")), reason="no trained weights shipped")
+def test_trained_network_does_not_lose_on_a_held_out_grid():
+    """A long-diameter graph the network was not trained on (1536 x 1024
+    grid; training grids are 512^2, 1024 x 256 and 2048 x 1024): every level
+    is a small top-down step, where the learned switch must cost no more than
+    the reference heuristic (its decision is certified from the last
+    evaluation, so the network runs on a few dozen of the ~2,500 levels)."""
+    from xbfs_b200 import learned
+    w, _ = learned.load()
+    learned.install(w)
+    try:
+        res = learned.evaluate([("grid", 1536, 1024)], sources=4, seed=3, reps=3, policies=("heuristic", "mlp"))
+    finally:
+        learned.install(None)
+    r = res[str(("grid", 1536, 1024))]
+    gain = r["heuristic"]["ms"] / r["mlp"]["ms"]
+    print(f"learned switch vs heuristic on the 1536 x 1024 grid: {gain:.3f}x "
+          f"({r['heuristic']['ms']:.2f} ms -> {r['mlp']['ms']:.2f} ms)")
+    assert gain >= 1.0

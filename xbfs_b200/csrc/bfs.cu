@@ -67,6 +67,11 @@ constexpr int kTE = kBlock * kK;    // edges per gather round
 // probes read at random (doubling the staging areas cost ~30% on the
 // bottom-up level of R-MAT scale 23 through the smaller L1).
 constexpr int kWin = kTE;           // shared window / tile list capacity
+constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: up to this many kTE per round
+#ifndef XBFS_TD_ILP
+#define XBFS_TD_ILP 4
+#endif
+constexpr int kTdIlp = XBFS_TD_ILP; // edges per thread in flight in the barrier-free top-down loops
 constexpr int kCap = 1024;          // staging capacity, small and medium bins
 constexpr int kCapL = 256;          // staging capacity, large bin
 constexpr int kFlushAt = kCap - kTE;  // a round adds at most kTE winners: flush before each
@@ -327,7 +332,6 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane, float* ca
   const float* B2 = W2T + 1024;
   const float* W3 = B2 + 32;
   const float* B3 = W3 + 96;
-  const float* P = B3 + 3;
   float f = 0.f;
   if (lane < 8) {
     const float r = raw[lane];
@@ -336,7 +340,6 @@ __device__ int mlp_decide(const float* sw, const float* raw, int lane, float* ca
     else f = log1pf(r > 0.f ? r : 0.f);
     f = (f - mean[lane]) / sd[lane];
   }
-  (void)P;
   float a = B1[lane];
 #pragma unroll
   for (int i = 0; i < 8; ++i) a = fmaf(W1T[i * 32 + lane], __shfl_sync(0xffffffffu, f, i), a);
@@ -559,6 +562,59 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
   }
   __syncthreads();
   unsigned s = (unsigned)sm.next_s;
+  if (!enq) {
+    // bitmap output: nothing is staged, so a round may take up to
+    // kRoundsNoStage x kTE edges (as far as the window's owners reach),
+    // expanded kTdIlp edges per thread at a time with their visited words
+    // loaded together: a quarter of the block barriers of the staged rounds
+    constexpr unsigned long long kR = (unsigned long long)kRoundsNoStage * kTE;
+    for (unsigned long long r = lo; r < hi;) {
+      unsigned long long rhi = (r + kR < hi) ? r + kR : hi;
+      if (s + kWin < cnt) {
+        const unsigned long long w_end = in.eb[s + kWin];  // the window holds owners s .. s + kWin
+        if (w_end < rhi) rhi = w_end;
+      }
+      for (int i = threadIdx.x; i <= kWin; i += kBlock) {
+        const unsigned slot = s + (unsigned)i;
+        unsigned e0 = 0xffffffffu;
+        if (slot < cnt) {
+          const unsigned x = in.eb[slot];
+          if ((unsigned long long)x < rhi) {
+            e0 = x;
+            sm.wu[i] = in.ids[slot];
+            sm.wbeg[i] = in.bg[slot];
+          }
+        }
+        sm.web[i] = e0;
+      }
+      __syncthreads();
+      for (unsigned long long e0 = r + threadIdx.x; e0 < rhi; e0 += (unsigned long long)kTdIlp * kBlock) {
+        int v[kTdIlp], u[kTdIlp];
+#pragma unroll
+        for (int k = 0; k < kTdIlp; ++k) {
+          const unsigned long long e = e0 + (unsigned long long)k * kBlock;
+          v[k] = -1;
+          u[k] = 0;
+          if (e < rhi) {
+            const int a = smem_owner(sm.web, kWin + 1, e);
+            v[k] = ld_stream_i32(p.csr + sm.wbeg[a] + (long long)(e - sm.web[a]));
+            u[k] = sm.wu[a];
+          }
+        }
+        uint32_t vw[kTdIlp];
+#pragma unroll
+        for (int k = 0; k < kTdIlp; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
+#pragma unroll
+        for (int k = 0; k < kTdIlp; ++k)
+          if (v[k] >= 0 && !((vw[k] >> (v[k] & 31)) & 1u)) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, false, fbn, true);
+      }
+      if (threadIdx.x == 0 && rhi < hi) sm.next_s = (int)(s + smem_owner(sm.web, kWin + 1, rhi));
+      __syncthreads();
+      s = (unsigned)sm.next_s;
+      r = rhi;
+    }
+    return;
+  }
   for (unsigned long long r = lo; r < hi; r += kTE) {
     const unsigned long long rhi = (r + kTE < hi) ? r + kTE : hi;
     for (int i = threadIdx.x; i <= kTE; i += kBlock) {
@@ -824,13 +880,13 @@ __device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc
     // 3. edge-balanced expansion of the tile
     if (!enq) {
       // bitmap output: nothing is staged, so the rounds need no block
-      // barrier; each thread keeps four edges in flight (their neighbour
-      // ids, then the visited words of all four) and claims only the
+      // barrier; each thread keeps kTdIlp edges in flight (their neighbour
+      // ids, then the visited words of all of them) and claims only the
       // targets that looked unvisited
-      for (long long e0 = threadIdx.x; e0 < T; e0 += 4 * kBlock) {
-        int v[4], u[4];
+      for (long long e0 = threadIdx.x; e0 < T; e0 += (long long)kTdIlp * kBlock) {
+        int v[kTdIlp], u[kTdIlp];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < kTdIlp; ++k) {
           const long long e = e0 + (long long)k * kBlock;
           v[k] = -1;
           u[k] = 0;
@@ -840,11 +896,11 @@ __device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc
             u[k] = sm.wu[a];
           }
         }
-        uint32_t vw[4];
+        uint32_t vw[kTdIlp];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
+        for (int k = 0; k < kTdIlp; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
+        for (int k = 0; k < kTdIlp; ++k)
           if (v[k] >= 0 && !((vw[k] >> (v[k] & 31)) & 1u)) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, false, fbn, true);
       }
       __syncthreads();  // the next chunk rewrites the window
@@ -1147,7 +1203,7 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
 #define XBFS_BU_WORDS 2
 #endif
 #ifndef XBFS_BU_FIRST
-#define XBFS_BU_FIRST 4
+#define XBFS_BU_FIRST 2
 #endif
 constexpr int kBuWords = XBFS_BU_WORDS, kBuFirst = XBFS_BU_FIRST, kBuMore = 8;
 constexpr int kBuQueue = 2 * kCap;
@@ -1868,7 +1924,6 @@ xbfs_status bfs_single(Graph* g, int32_t src, int32_t* levels, int32_t* parents,
   size_t smem = 0;
   int grid = 0;
   if ((st = setup_params(g, o, d_levels, d_parents, p, &kfn, &smem, &grid))) return st;
-  const bool par_on = parents != nullptr;
 
   // ---- one launch: it sets up the traversal state itself (init_traversal);
   // only the control block, which holds the launch's grid barrier, is
