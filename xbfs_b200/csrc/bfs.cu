@@ -514,6 +514,44 @@ __device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& 
   }
 }
 
+// Top-down claims of kTdIlp targets v[k] (reached from u[k]; v[k] < 0: none)
+// for level L+1 with bitmap output, all in flight together: the visited
+// words, then the atomics of the targets that looked unvisited with their
+// CSR offsets (for the frontier statistics), then the winners' writes. Same
+// rules as claim_td; only the independent loads and atomics of different
+// targets overlap instead of one target's chain after another's.
+template <bool PAR>
+__device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int (&v)[kTdIlp], const int (&u)[kTdIlp],
+                                            int L, uint32_t* fbn) {
+  uint32_t vw[kTdIlp];
+#pragma unroll
+  for (int k = 0; k < kTdIlp; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
+  bool cand[kTdIlp];
+  long long b0[kTdIlp], b1[kTdIlp];
+  uint32_t old[kTdIlp];
+#pragma unroll
+  for (int k = 0; k < kTdIlp; ++k) {
+    cand[k] = v[k] >= 0 && !((vw[k] >> (v[k] & 31)) & 1u);
+    b0[k] = 0;
+    b1[k] = 0;
+    old[k] = ~0u;
+    if (cand[k]) {
+      b0[k] = ld_nc_i64(p.beg + v[k]);
+      b1[k] = ld_nc_i64(p.beg + v[k] + 1);
+      old[k] = atomicOr(p.vis + (v[k] >> 5), 1u << (v[k] & 31));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kTdIlp; ++k) {
+    if (!cand[k] || ((old[k] >> (v[k] & 31)) & 1u)) continue;
+    p.levels[v[k]] = L + 1;
+    if (PAR) p.parents[v[k]] = u[k];
+    acc.n1 += 1;
+    acc.m1 += b1[k] - b0[k];
+    red_or_u32(fbn + (v[k] >> 5), 1u << (v[k] & 31));
+  }
+}
+
 // Warp-parallel search: last slot s in [0, cnt) with eb[s] <= key (eb strictly
 // increasing from eb[0] = 0 <= key). Called by a full warp.
 __device__ int find_owner(const unsigned* eb, unsigned cnt, unsigned long long key) {
@@ -601,12 +639,7 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
             u[k] = sm.wu[a];
           }
         }
-        uint32_t vw[kTdIlp];
-#pragma unroll
-        for (int k = 0; k < kTdIlp; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
-#pragma unroll
-        for (int k = 0; k < kTdIlp; ++k)
-          if (v[k] >= 0 && !((vw[k] >> (v[k] & 31)) & 1u)) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, false, fbn, true);
+        claim_batch<PAR>(p, acc, v, u, L, fbn);
       }
       if (threadIdx.x == 0 && rhi < hi) sm.next_s = (int)(s + smem_owner(sm.web, kWin + 1, rhi));
       __syncthreads();
@@ -896,12 +929,7 @@ __device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc
             u[k] = sm.wu[a];
           }
         }
-        uint32_t vw[kTdIlp];
-#pragma unroll
-        for (int k = 0; k < kTdIlp; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
-#pragma unroll
-        for (int k = 0; k < kTdIlp; ++k)
-          if (v[k] >= 0 && !((vw[k] >> (v[k] & 31)) & 1u)) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, false, fbn, true);
+        claim_batch<PAR>(p, acc, v, u, L, fbn);
       }
       __syncthreads();  // the next chunk rewrites the window
     } else {
