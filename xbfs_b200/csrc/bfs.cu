@@ -516,40 +516,43 @@ __device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& 
 
 // Top-down claims of kTdIlp targets v[k] (reached from u[k]; v[k] < 0: none)
 // for level L+1 with bitmap output, all in flight together: the visited
-// words, then the atomics of the targets that looked unvisited with their
-// CSR offsets (for the frontier statistics), then the winners' writes. Same
-// rules as claim_td; only the independent loads and atomics of different
-// targets overlap instead of one target's chain after another's.
+// words, then the atomics of the targets that looked unvisited, then the
+// winners' writes and CSR offsets (for the frontier statistics). Same rules
+// as claim_td; the independent loads and atomics of different targets
+// overlap, and the offsets are read for winners only: on a level where many
+// edges race for the same fresh targets, reading them for every candidate
+// (claim_td's speculative order) costs a random DRAM sector per losing edge.
 template <bool PAR>
 __device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int (&v)[kTdIlp], const int (&u)[kTdIlp],
                                             int L, uint32_t* fbn) {
   uint32_t vw[kTdIlp];
 #pragma unroll
   for (int k = 0; k < kTdIlp; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
-  bool cand[kTdIlp];
-  long long b0[kTdIlp], b1[kTdIlp];
-  uint32_t old[kTdIlp];
+  bool win[kTdIlp];
 #pragma unroll
   for (int k = 0; k < kTdIlp; ++k) {
-    cand[k] = v[k] >= 0 && !((vw[k] >> (v[k] & 31)) & 1u);
-    b0[k] = 0;
-    b1[k] = 0;
-    old[k] = ~0u;
-    if (cand[k]) {
-      b0[k] = ld_nc_i64(p.beg + v[k]);
-      b1[k] = ld_nc_i64(p.beg + v[k] + 1);
-      old[k] = atomicOr(p.vis + (v[k] >> 5), 1u << (v[k] & 31));
+    win[k] = false;
+    if (v[k] >= 0 && !((vw[k] >> (v[k] & 31)) & 1u)) {
+      const uint32_t bit = 1u << (v[k] & 31);
+      win[k] = (atomicOr(p.vis + (v[k] >> 5), bit) & bit) == 0;
     }
   }
+  long long d[kTdIlp];
 #pragma unroll
   for (int k = 0; k < kTdIlp; ++k) {
-    if (!cand[k] || ((old[k] >> (v[k] & 31)) & 1u)) continue;
+    d[k] = 0;
+    if (!win[k]) continue;
     p.levels[v[k]] = L + 1;
     if (PAR) p.parents[v[k]] = u[k];
-    acc.n1 += 1;
-    acc.m1 += b1[k] - b0[k];
     red_or_u32(fbn + (v[k] >> 5), 1u << (v[k] & 31));
+    d[k] = ld_nc_i64(p.beg + v[k] + 1) - ld_nc_i64(p.beg + v[k]);
   }
+#pragma unroll
+  for (int k = 0; k < kTdIlp; ++k)
+    if (win[k]) {
+      acc.n1 += 1;
+      acc.m1 += d[k];
+    }
 }
 
 // Warp-parallel search: last slot s in [0, cnt) with eb[s] <= key (eb strictly
