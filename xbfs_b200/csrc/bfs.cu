@@ -203,6 +203,8 @@ struct __align__(16) Smem {
   int bu_next;
   int bu_n;
   int bu_dense;                 // this level's unvisited vertices are at least a quarter of V
+  int qside_ok;                 // few unvisited vertices and no early next-frontier entries: a
+                                // top-down level with bitmap output also fills the next queue
   int chunk;
   unsigned long long bins[3];   // F_L bin counters, read once per level
   long long pend_next;          // F_{L+1} entries already found (async bottom-up)
@@ -487,7 +489,7 @@ struct Acc {
 // whether this thread wins.
 template <bool PAR>
 __device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& q, Acc& acc, int v, int u,
-                                         int L, bool enq, uint32_t* fbn, bool spec) {
+                                         int L, bool enq, uint32_t* fbn, bool spec, bool qside = false) {
   const uint32_t word = (uint32_t)v >> 5, bit = 1u << (v & 31);
   long long b0 = 0, b1 = 0;
   if (spec) {
@@ -511,6 +513,10 @@ __device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& 
     if (d > 0) stage(sm, q, bin_of(d, p.small_max, p.medium_max), v, d, b0);
   } else {
     red_or_u32(fbn + word, bit);
+    if (qside && d > 0) {
+      const int bin = bin_of(d, p.small_max, p.medium_max);
+      direct_enqueue(q.b[bin], &q.ctr[bin], v, d, b0);
+    }
   }
 }
 
@@ -524,7 +530,7 @@ __device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& 
 // (claim_td's speculative order) costs a random DRAM sector per losing edge.
 template <bool PAR>
 __device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int (&v)[kTdIlp], const int (&u)[kTdIlp],
-                                            int L, uint32_t* fbn) {
+                                            int L, uint32_t* fbn, const QOut& q, bool qside) {
   uint32_t vw[kTdIlp];
 #pragma unroll
   for (int k = 0; k < kTdIlp; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
@@ -537,21 +543,27 @@ __device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int
       win[k] = (atomicOr(p.vis + (v[k] >> 5), bit) & bit) == 0;
     }
   }
-  long long d[kTdIlp];
+  long long b0[kTdIlp], d[kTdIlp];
 #pragma unroll
   for (int k = 0; k < kTdIlp; ++k) {
+    b0[k] = 0;
     d[k] = 0;
     if (!win[k]) continue;
     p.levels[v[k]] = L + 1;
     if (PAR) p.parents[v[k]] = u[k];
     red_or_u32(fbn + (v[k] >> 5), 1u << (v[k] & 31));
-    d[k] = ld_nc_i64(p.beg + v[k] + 1) - ld_nc_i64(p.beg + v[k]);
+    b0[k] = ld_nc_i64(p.beg + v[k]);
+    d[k] = ld_nc_i64(p.beg + v[k] + 1) - b0[k];
   }
 #pragma unroll
   for (int k = 0; k < kTdIlp; ++k)
     if (win[k]) {
       acc.n1 += 1;
       acc.m1 += d[k];
+      if (qside && d[k] > 0) {
+        const int bin = bin_of(d[k], p.small_max, p.medium_max);
+        direct_enqueue(q.b[bin], &q.ctr[bin], v[k], d[k], b0[k]);
+      }
     }
 }
 
@@ -591,7 +603,7 @@ __device__ __forceinline__ int smem_owner(const unsigned* web, int n, unsigned l
 // and large bins, and the heavy list of a fused sweep).
 template <bool PAR>
 __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
-                           unsigned long long M, int L, bool enq, uint32_t* fbn) {
+                           unsigned long long M, int L, bool enq, uint32_t* fbn, bool qside) {
   if (cnt == 0 || M == 0) return;
   const bool spec = sm.spec != 0;
   const unsigned long long G = gridDim.x, b = blockIdx.x;
@@ -642,7 +654,7 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
             u[k] = sm.wu[a];
           }
         }
-        claim_batch<PAR>(p, acc, v, u, L, fbn);
+        claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
       }
       if (threadIdx.x == 0 && rhi < hi) sm.next_s = (int)(s + smem_owner(sm.web, kWin + 1, rhi));
       __syncthreads();
@@ -692,7 +704,7 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
 // small_max, so shares of many entries carry similar numbers of edges.
 template <bool PAR>
 __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
-                               unsigned long long M, int L, bool enq, uint32_t* fbn) {
+                               unsigned long long M, int L, bool enq, uint32_t* fbn, bool qside) {
   if (cnt == 0) return;
   const bool spec = sm.spec != 0;
   const unsigned long long G = gridDim.x, b = blockIdx.x;
@@ -731,7 +743,7 @@ __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& ac
       }
 #pragma unroll
       for (int k = 0; k < kK; ++k)
-        if (v[k] >= 0) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, enq, fbn, spec);
+        if (v[k] >= 0) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, enq, fbn, spec, qside);
       __syncthreads();
       if (enq && need_flush(sm)) flush(sm, q);
     }
@@ -748,7 +760,7 @@ __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& ac
 template <bool PAR>
 __device__ void gather_entries_warp(const Params& p, const QOut& q, const QBin& in, unsigned cnt,
                                     unsigned long long M, unsigned i0, unsigned i1, int L, bool enq, uint32_t* fbn,
-                                    bool spec, FDesc* f1) {
+                                    bool spec, FDesc* f1, bool qside) {
   const int lane = threadIdx.x & 31;
   const unsigned i = i0 + lane;
   const bool own = i < i1;
@@ -806,7 +818,13 @@ __device__ void gather_entries_warp(const Params& p, const QOut& q, const QBin& 
         }
         n1 += 1;
         m1 += b1 - b0;
-        if (!enq) red_or_u32(fbn + word, bit);
+        if (!enq) {
+          red_or_u32(fbn + word, bit);
+          if (qside && b1 > b0) {
+            const int qb = bin_of(b1 - b0, p.small_max, p.medium_max);
+            direct_enqueue(q.b[qb], &q.ctr[qb], v, b1 - b0, b0);
+          }
+        }
       }
     }
     if (enq) {
@@ -846,7 +864,7 @@ __device__ void gather_entries_warp(const Params& p, const QOut& q, const QBin& 
 // list expanded grid-wide after the barrier.
 template <bool PAR>
 __device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc, const uint32_t* fbc, int L,
-                              bool enq, uint32_t* fbn, int par) {
+                              bool enq, uint32_t* fbn, int par, bool qside) {
   const bool spec = sm.spec != 0;
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
@@ -932,7 +950,7 @@ __device__ void expand_bitmap(const Params& p, Smem& sm, const QOut& q, Acc& acc
             u[k] = sm.wu[a];
           }
         }
-        claim_batch<PAR>(p, acc, v, u, L, fbn);
+        claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
       }
       __syncthreads();  // the next chunk rewrites the window
     } else {
@@ -1577,6 +1595,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         if (n_u < 0) n_u = 0;
         if (m_u < 0) m_u = 0;
         sm.bu_dense = (n_u * 4 >= p.V) ? 1 : 0;
+        sm.qside_ok = (pn == 0 && n_u * 64 <= p.V) ? 1 : 0;
         switch (p.policy) {
           case XBFS_POLICY_FORCED: {
             const long long i = L < p.n_forced ? L : p.n_forced - 1;
@@ -1655,6 +1674,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
 
     if (S == XBFS_TD_QUEUE || S == XBFS_TD_SCAN) {
       const bool enq = (S == XBFS_TD_QUEUE) && (sm.pend_next == 0);
+      // A top-down level with bitmap output (single scan, or a queue level
+      // after an asynchronous bottom-up) can only have as many winners as
+      // there are unvisited vertices; when those are few, the winners also
+      // go straight into the next level's binned queue (one atomic each),
+      // so a small next level expands the queue instead of sweeping the
+      // bitmap (the bitmap stays valid too)
+      const bool qside = !enq && sm.qside_ok;
       QOut qo;
       for (int b2 = 0; b2 < 3; ++b2) qo.b[b2] = p.q[par ^ 1][b2];
       qo.ctr = F1->bin;
@@ -1667,16 +1693,18 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       const bool tiny = q_valid && (sm.bins[1] & kCountMask) == 0 && (sm.bins[2] & kCountMask) == 0 && i1 - i0 <= 32;
       if (tiny) {
         if (threadIdx.x < 32 && i1 > i0)
-          gather_entries_warp<PAR>(p, qo, p.q[par][0], cnt0, pk0 >> 31, i0, i1, (int)L, enq, fbn, sm.spec != 0, F1);
+          gather_entries_warp<PAR>(p, qo, p.q[par][0], cnt0, pk0 >> 31, i0, i1, (int)L, enq, fbn, sm.spec != 0, F1,
+                                   qside);
       } else {
         if (q_valid) {
           for (int bin = 2; bin >= 1; --bin) {
             const unsigned long long pk = sm.bins[bin];
-            gather_bin<PAR>(p, sm, qo, acc, p.q[par][bin], (unsigned)(pk & kCountMask), pk >> 31, (int)L, enq, fbn);
+            gather_bin<PAR>(p, sm, qo, acc, p.q[par][bin], (unsigned)(pk & kCountMask), pk >> 31, (int)L, enq, fbn,
+                            qside);
           }
-          gather_entries<PAR>(p, sm, qo, acc, p.q[par][0], cnt0, pk0 >> 31, (int)L, enq, fbn);
+          gather_entries<PAR>(p, sm, qo, acc, p.q[par][0], cnt0, pk0 >> 31, (int)L, enq, fbn, qside);
         } else {
-          expand_bitmap<PAR>(p, sm, qo, acc, fbc, (int)L, enq, fbn, par);
+          expand_bitmap<PAR>(p, sm, qo, acc, fbc, (int)L, enq, fbn, par, qside);
         }
         if (enq) flush(sm, qo);
         publish_acc(sm, acc, F1, nullptr);
@@ -1687,13 +1715,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         // (the list is complete only after the barrier; usually it is empty)
         const unsigned long long hk = ld_cg_u64(&ctl->heavy[par]);
         if ((hk & kCountMask) != 0) {
-          gather_bin<PAR>(p, sm, qo, acc, p.heavy, (unsigned)(hk & kCountMask), hk >> 31, (int)L, enq, fbn);
+          gather_bin<PAR>(p, sm, qo, acc, p.heavy, (unsigned)(hk & kCountMask), hk >> 31, (int)L, enq, fbn, qside);
           if (enq) flush(sm, qo);
           publish_acc(sm, acc, F1, nullptr);
           if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
         }
       }
-      q_valid = enq;
+      q_valid = enq || qside;
       b_valid = !enq;
       if (!enq) dirty |= 1u << ((L + 1) & 3);
     } else {
