@@ -66,7 +66,10 @@ constexpr int kTE = kBlock * kK;    // edges per gather round
 // which caches the frontier-bitmap words and CSR offsets that bottom-up
 // probes read at random (doubling the staging areas cost ~30% on the
 // bottom-up level of R-MAT scale 23 through the smaller L1).
-constexpr int kWin = kTE;           // shared window / tile list capacity
+#ifndef XBFS_WIN_FACTOR
+#define XBFS_WIN_FACTOR 1
+#endif
+constexpr int kWin = XBFS_WIN_FACTOR * kTE;  // shared window / tile list capacity (at least kTE)
 constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: up to this many kTE per round
 #ifndef XBFS_TD_ILP
 #define XBFS_TD_ILP 4
@@ -178,6 +181,7 @@ struct PolicyState {
 struct LoopState {
   PolicyState ps;
   long long vis_n, vis_m;  // sums over frontiers <= L
+  long long pend_q_for;    // frontier whose early (asynchronous bottom-up) entries are also queued
   // statistics of the whole traversal (used by block 0)
   unsigned long long st_reached, st_msum, st_async;
   int st_strat[3];
@@ -203,8 +207,9 @@ struct __align__(16) Smem {
   int bu_next;
   int bu_n;
   int bu_dense;                 // this level's unvisited vertices are at least a quarter of V
-  int qside_ok;                 // few unvisited vertices and no early next-frontier entries: a
-                                // top-down level with bitmap output also fills the next queue
+  int qside_ok;                 // few unvisited vertices and every early next-frontier entry queued:
+                                // a top-down level with bitmap output also fills the next queue
+  int asyncq_ok;                // few unvisited vertices: asynchronous bottom-up winners are queued
   int chunk;
   unsigned long long bins[3];   // F_L bin counters, read once per level
   long long pend_next;          // F_{L+1} entries already found (async bottom-up)
@@ -227,6 +232,7 @@ struct ResumeState {
   int q_valid, b_valid;
   unsigned dirty;
   long long vis_n, vis_m;
+  long long pend_q_for;
   PolicyState ps;
 };
 
@@ -1057,6 +1063,15 @@ __device__ __forceinline__ void probe_pair(const Params& p, const uint32_t* fbc,
   }
 }
 
+// A level-(L+2) winner of the asynchronous bottom-up rule into frontier
+// L+2's binned queue (q2 = nullptr: not queued this level).
+__device__ __forceinline__ void queue_early(const Params& p, const QOut* q2, int v, long long d, long long b0) {
+  if (q2 && d > 0) {
+    const int bin = bin_of(d, p.small_max, p.medium_max);
+    direct_enqueue(q2->b[bin], &q2->ctr[bin], v, d, b0);
+  }
+}
+
 // Publishes a warp's bottom-up results for 32 consecutive entries of a sorted
 // list: vertices sharing a bitmap word sit in adjacent lanes, so their bits
 // are ORed along each run of equal words and the run's first lane issues one
@@ -1093,7 +1108,7 @@ __device__ __forceinline__ void bu_publish_words(const Params& p, uint32_t* fbn,
 // (most vertices find a parent among the first few).
 template <bool PAR, bool ASYNC>
 __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
-                          uint32_t* fbn2) {
+                          uint32_t* fbn2, const QOut* q2) {
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
@@ -1165,6 +1180,7 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
             m2 = bit;
             acc.n2 += 1;
             acc.m2 += ee[j] - eb[j];
+            queue_early(p, q2, v[j], ee[j] - eb[j], eb[j]);
           }
         }
         bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, m2, v[j] >= 0);
@@ -1209,6 +1225,7 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
         m2 = bit;
         acc.n2 += 1;
         acc.m2 += e1 - e0;
+        queue_early(p, q2, v, e1 - e0, e0);
       }
     }
     // The warp's 32 vertices are consecutive entries of a sorted list, so
@@ -1259,7 +1276,7 @@ constexpr int kBuQueue = 2 * kCap;
 
 template <bool PAR, bool ASYNC>
 __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
-                                uint32_t* fbn2) {
+                                uint32_t* fbn2, const QOut* q2) {
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
@@ -1346,6 +1363,7 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
         if (PAR) p.parents[v] = found2;
         acc.n2 += 1;
         acc.m2 += d;
+        queue_early(p, q2, v, d, e[k]);
       }
       const uint32_t m1 = __ballot_sync(0xffffffffu, got1);
       const uint32_t m2 = __ballot_sync(0xffffffffu, got2);
@@ -1386,6 +1404,7 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
         m2 = bit;
         acc.n2 += 1;
         acc.m2 += e1 - e0;
+        queue_early(p, q2, v, e1 - e0, e0);
       }
     }
     bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, m2, i < nq);
@@ -1513,6 +1532,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
     ls.ps.prev_strategy = XBFS_TD_QUEUE;
     ls.vis_n = 0;
     ls.vis_m = 0;
+    ls.pend_q_for = -1;
     ls.st_reached = 0;
     ls.st_msum = 0;
     ls.st_async = 0;
@@ -1521,6 +1541,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       const ResumeState r = *p.rs;
       ls.vis_n = r.vis_n;
       ls.vis_m = r.vis_m;
+      ls.pend_q_for = r.pend_q_for;
       ls.ps = r.ps;
     }
   }
@@ -1557,6 +1578,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         r.dirty = dirty;
         r.vis_n = ls.vis_n;
         r.vis_m = ls.vis_m;
+        r.pend_q_for = ls.pend_q_for;
         r.ps = ls.ps;
         *p.rs = r;
       }
@@ -1595,7 +1617,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         if (n_u < 0) n_u = 0;
         if (m_u < 0) m_u = 0;
         sm.bu_dense = (n_u * 4 >= p.V) ? 1 : 0;
-        sm.qside_ok = (pn == 0 && n_u * 64 <= p.V) ? 1 : 0;
+        sm.asyncq_ok = (n_u * 64 <= p.V) ? 1 : 0;
+        sm.qside_ok = (n_u * 64 <= p.V && (pn == 0 || ls.pend_q_for == L + 1)) ? 1 : 0;
         switch (p.policy) {
           case XBFS_POLICY_FORCED: {
             const long long i = L < p.n_forced ? L : p.n_forced - 1;
@@ -1734,15 +1757,24 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       // bottom-up level of a power-law graph), else over the compacted list
       // of unvisited vertices (few per bitmap word: most lanes of a word
       // would idle)
+      // with few unvisited vertices, level L+2 winners of the asynchronous
+      // rule also go into frontier L+2's queue (whose counters this level
+      // may use: nothing else writes them before level L+1), so the
+      // top-down level L+1 can complete that queue beside its bitmap
+      QOut qo2;
+      for (int b2 = 0; b2 < 3; ++b2) qo2.b[b2] = p.q[par][b2];
+      qo2.ctr = F2->bin;
+      const QOut* q2 = (p.async_bu && sm.asyncq_ok) ? &qo2 : nullptr;
+      if (threadIdx.x == 0 && q2) ls.pend_q_for = L + 2;
       if (p.bu_mode == 5 || (p.bu_mode == 0 && sm.bu_dense)) {
         if (p.async_bu)
-          bottom_up_words<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+          bottom_up_words<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2, q2);
         else
-          bottom_up_words<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+          bottom_up_words<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2, nullptr);
       } else if (p.async_bu) {
-        bottom_up<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+        bottom_up<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2, q2);
       } else {
-        bottom_up<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+        bottom_up<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2, nullptr);
       }
       publish_acc(sm, acc, F1, F2);
       if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
