@@ -71,6 +71,11 @@ constexpr int kTE = kBlock * kK;    // edges per gather round
 #endif
 constexpr int kWin = XBFS_WIN_FACTOR * kTE;  // shared window / tile list capacity (at least kTE)
 constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: up to this many kTE per round
+// Asynchronous bottom-up winners of sparse (list-probing) bottom-up levels
+// go into frontier L+2's queue (1) or only into its bitmap (0).
+#ifndef XBFS_ASYNC_QUEUE
+#define XBFS_ASYNC_QUEUE 1
+#endif
 #ifndef XBFS_TD_ILP
 #define XBFS_TD_ILP 4
 #endif
@@ -209,7 +214,7 @@ struct __align__(16) Smem {
   int bu_dense;                 // this level's unvisited vertices are at least a quarter of V
   int qside_ok;                 // few unvisited vertices and every early next-frontier entry queued:
                                 // a top-down level with bitmap output also fills the next queue
-  int asyncq_ok;                // few unvisited vertices: asynchronous bottom-up winners are queued
+  int asyncq_ok;                // a sparse bottom-up level: its asynchronous winners are queued
   int chunk;
   unsigned long long bins[3];   // F_L bin counters, read once per level
   long long pend_next;          // F_{L+1} entries already found (async bottom-up)
@@ -1063,12 +1068,31 @@ __device__ __forceinline__ void probe_pair(const Params& p, const uint32_t* fbc,
   }
 }
 
-// A level-(L+2) winner of the asynchronous bottom-up rule into frontier
-// L+2's binned queue (q2 = nullptr: not queued this level).
-__device__ __forceinline__ void queue_early(const Params& p, const QOut* q2, int v, long long d, long long b0) {
-  if (q2 && d > 0) {
-    const int bin = bin_of(d, p.small_max, p.medium_max);
-    direct_enqueue(q2->b[bin], &q2->ctr[bin], v, d, b0);
+// Level-(L+2) winners of the asynchronous bottom-up rule (lanes with `have`)
+// into frontier L+2's binned queue: per bin one packed atomic for the warp
+// (edges << 31 | count), entries at consecutive slots. Called by a full warp.
+__device__ __forceinline__ void queue_early_warp(const Params& p, const QOut& q2, bool have, int v, long long d,
+                                                 long long b0) {
+  const int lane = threadIdx.x & 31;
+  have = have && d > 0;
+  if (!__ballot_sync(0xffffffffu, have)) return;
+  const int bin = have ? bin_of(d, p.small_max, p.medium_max) : -1;
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    const bool mine = bin == b;
+    const unsigned mask = __ballot_sync(0xffffffffu, mine);
+    if (!mask) continue;
+    const long long dd = mine ? d : 0;
+    const long long inc = warp_inclusive_scan(dd);
+    unsigned long long old = 0;
+    if (lane == 31) old = atomicAdd(&q2.ctr[b], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
+    old = __shfl_sync(0xffffffffu, old, 31);
+    if (mine) {
+      const unsigned long long slot = (old & kCountMask) + __popc(mask & ((1u << lane) - 1));
+      q2.b[b].ids[slot] = v;
+      q2.b[b].eb[slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - dd));
+      q2.b[b].bg[slot] = b0;
+    }
   }
 }
 
@@ -1108,7 +1132,7 @@ __device__ __forceinline__ void bu_publish_words(const Params& p, uint32_t* fbn,
 // (most vertices find a parent among the first few).
 template <bool PAR, bool ASYNC>
 __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
-                          uint32_t* fbn2, const QOut* q2) {
+                          uint32_t* fbn2, const QOut& q2, bool asyncq) {
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
@@ -1180,9 +1204,9 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
             m2 = bit;
             acc.n2 += 1;
             acc.m2 += ee[j] - eb[j];
-            queue_early(p, q2, v[j], ee[j] - eb[j], eb[j]);
           }
         }
+        if (ASYNC && asyncq) queue_early_warp(p, q2, m2 != 0, v[j], ee[j] - eb[j], eb[j]);
         bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, m2, v[j] >= 0);
       }
     }
@@ -1195,9 +1219,12 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
     if (base >= n) break;
     const int i = base + lane;
     uint32_t word = 0xffffffffu, m1 = 0, m2 = 0;  // bitmap word of this lane's vertex, bits to set
+    int v = -1;
+    long long e0 = 0, e1 = 0;
     if (i < n) {
-      const int v = list[i];
-      const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
+      v = list[i];
+      e0 = ld_nc_i64(p.beg + v);
+      e1 = ld_nc_i64(p.beg + v + 1);
       int found = -1, found2 = -1;
       long long e = e0;
       if (p.bu_mode == 2) {  // four at a time, streaming loads
@@ -1225,9 +1252,9 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
         m2 = bit;
         acc.n2 += 1;
         acc.m2 += e1 - e0;
-        queue_early(p, q2, v, e1 - e0, e0);
       }
     }
+    if (ASYNC && asyncq) queue_early_warp(p, q2, m2 != 0, v, e1 - e0, e0);
     // The warp's 32 vertices are consecutive entries of a sorted list, so
     // vertices sharing a bitmap word sit in adjacent lanes: OR their bits
     // along each run of equal words and let the run's first lane publish
@@ -1276,7 +1303,7 @@ constexpr int kBuQueue = 2 * kCap;
 
 template <bool PAR, bool ASYNC>
 __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
-                                uint32_t* fbn2, const QOut* q2) {
+                                uint32_t* fbn2) {
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
@@ -1363,7 +1390,6 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
         if (PAR) p.parents[v] = found2;
         acc.n2 += 1;
         acc.m2 += d;
-        queue_early(p, q2, v, d, e[k]);
       }
       const uint32_t m1 = __ballot_sync(0xffffffffu, got1);
       const uint32_t m2 = __ballot_sync(0xffffffffu, got2);
@@ -1404,7 +1430,6 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
         m2 = bit;
         acc.n2 += 1;
         acc.m2 += e1 - e0;
-        queue_early(p, q2, v, e1 - e0, e0);
       }
     }
     bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, m2, i < nq);
@@ -1617,7 +1642,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         if (n_u < 0) n_u = 0;
         if (m_u < 0) m_u = 0;
         sm.bu_dense = (n_u * 4 >= p.V) ? 1 : 0;
-        sm.asyncq_ok = (n_u * 64 <= p.V) ? 1 : 0;
+        sm.asyncq_ok = (n_u * 4 < p.V) ? 1 : 0;
         sm.qside_ok = (n_u * 64 <= p.V && (pn == 0 || ls.pend_q_for == L + 1)) ? 1 : 0;
         switch (p.policy) {
           case XBFS_POLICY_FORCED: {
@@ -1757,24 +1782,26 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       // bottom-up level of a power-law graph), else over the compacted list
       // of unvisited vertices (few per bitmap word: most lanes of a word
       // would idle)
-      // with few unvisited vertices, level L+2 winners of the asynchronous
-      // rule also go into frontier L+2's queue (whose counters this level
-      // may use: nothing else writes them before level L+1), so the
-      // top-down level L+1 can complete that queue beside its bitmap
+      const bool words = p.bu_mode == 5 || (p.bu_mode == 0 && sm.bu_dense);
+      // on a sparse bottom-up level (list probing, few unvisited vertices)
+      // the level-(L+2) winners of the asynchronous rule also go into
+      // frontier L+2's queue, warp-aggregated (its counters are not used by
+      // anything else before level L+1), so a top-down level L+1 can
+      // complete that queue beside its bitmap
       QOut qo2;
       for (int b2 = 0; b2 < 3; ++b2) qo2.b[b2] = p.q[par][b2];
       qo2.ctr = F2->bin;
-      const QOut* q2 = (p.async_bu && sm.asyncq_ok) ? &qo2 : nullptr;
-      if (threadIdx.x == 0 && q2) ls.pend_q_for = L + 2;
-      if (p.bu_mode == 5 || (p.bu_mode == 0 && sm.bu_dense)) {
+      const bool asyncq = XBFS_ASYNC_QUEUE && p.async_bu && !words && sm.asyncq_ok;
+      if (threadIdx.x == 0 && asyncq) ls.pend_q_for = L + 2;
+      if (words) {
         if (p.async_bu)
-          bottom_up_words<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2, q2);
+          bottom_up_words<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
         else
-          bottom_up_words<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2, nullptr);
+          bottom_up_words<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
       } else if (p.async_bu) {
-        bottom_up<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2, q2);
+        bottom_up<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2, qo2, asyncq);
       } else {
-        bottom_up<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2, nullptr);
+        bottom_up<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2, qo2, false);
       }
       publish_acc(sm, acc, F1, F2);
       if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
