@@ -90,14 +90,21 @@ typedef struct xbfs_opts {
   float beamer_beta;    /*                     BU->TD when n_f < V/beta (24)   */
   int32_t bu_probe;     /* bottom-up probe shape: 0 = by density (default):
                            while unvisited vertices are at least V/4,
-                           word-parallel (5), else over a compacted list of
-                           them (4); 5 = word-parallel, each lane probing the
-                           first 4 neighbours of two vertices at once, longer
-                           scans deferred to a per-CTA queue; over the list:
-                           1 = 2, 4, then 8 neighbours at a time, streaming
-                           (L1 bypass); 2 = 4 at a time, streaming; 3 = two
-                           vertices per lane; 4 = 2, 4, then 8 at a time
-                           through L1 */
+                           word-parallel over head records (6), else over a
+                           compacted list of them, head record first and then
+                           the CSR segment (4 after the first three
+                           neighbours); 5 = word-parallel over CSR offsets,
+                           each lane probing the first 2 neighbours of two
+                           vertices at once, longer scans deferred to a
+                           per-CTA queue; 6 = the same over the graph's head
+                           records (first three neighbours and degree of each
+                           vertex, 16 bytes, written at upload and after
+                           xbfs_graph_sort_adjacency); over the list, CSR
+                           offsets only: 1 = 2, 4, then 8 neighbours at a
+                           time, streaming (L1 bypass); 2 = 4 at a time,
+                           streaming; 3 = two vertices per lane; 4 = 2, 4,
+                           then 8 at a time through L1. Other values:
+                           XBFS_ERR_INVALID_ARG */
   int32_t wait_timeout_us; /* bound of every device-side wait of a traversal
                               (grid barriers); 0 = 10 s. On expiry the call
                               returns XBFS_ERR_DEVICE_TIMEOUT */

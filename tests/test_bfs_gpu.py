@@ -224,10 +224,11 @@ def test_many_sources_pipelined_equal_single_calls(out, kind):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("bu_mode", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("bu_mode", [0, 1, 2, 3, 4, 5, 6])
 def test_bottom_up_probe_modes(bu_mode):
     """Every bottom-up probe shape gives the oracle's levels and a valid tree
-    (R-MAT with async bottom-up on and off, and a forced all-bottom-up run)."""
+    (R-MAT with async bottom-up on and off, and a forced all-bottom-up run);
+    modes 0 and 6 read the head records, the others the CSR offsets only."""
     beg, csr = gen_rmat_host(16, 16, 23)
     g = Graph.from_csr(beg, csr)
     for s in pick_sources(beg, 3, 8):
@@ -236,6 +237,38 @@ def test_bottom_up_probe_modes(bu_mode):
             r = g.bfs(int(s), want_parents=True, bu_mode=bu_mode, **kw)
             assert np.array_equal(r.levels, ref), (bu_mode, kw)
             assert oracle.check_tree(beg, csr, int(s), r.levels, r.parents) == 0
+    g.free()
+
+
+@pytest.mark.gpu
+def test_bottom_up_probe_mode_out_of_range_is_refused():
+    beg, csr = gen_rmat_host(10, 8, 2)
+    g = Graph.from_csr(beg, csr)
+    for m in (-1, 7):
+        with pytest.raises(XbfsError):
+            g.bfs(0, bu_mode=m)
+    g.free()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", ["degree", "id"])
+def test_head_records_follow_the_neighbour_order(order):
+    """The head records are rewritten when the neighbour order changes: an
+    all-bottom-up traversal after each re-order (probes start from the head
+    record, scans continue at the fourth CSR entry) matches the oracle on
+    the re-ordered CSR, in both word-parallel and list-based probing."""
+    beg, csr = gen_rmat_host(14, 8, 77)
+    g = Graph.from_csr(beg, csr)
+    g.sort_adjacency("degree")
+    if order == "id":
+        g.sort_adjacency("id")
+    b2, c2 = g.download()
+    for s in pick_sources(b2, 4, 5):
+        ref = oracle.bfs_queue(b2, c2, int(s))
+        for mode in (0, 6):
+            r = g.bfs(int(s), want_parents=True, bu_mode=mode, policy="forced", forced=["td_queue", "bu"])
+            assert np.array_equal(r.levels, ref), (order, mode)
+            assert oracle.check_tree(b2, c2, int(s), r.levels, r.parents) == 0
     g.free()
 
 

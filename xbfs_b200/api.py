@@ -54,7 +54,7 @@ class BfsOptions:
     beamer_alpha: float = 14.0
     beamer_beta: float = 24.0
     stream: int = 0
-    bu_mode: int = 0   # bottom-up probe shape (xbfs_opts.bu_probe): 0 = by density (default), 5 = word-parallel, 1-4 list-based
+    bu_mode: int = 0   # bottom-up probe shape (xbfs_opts.bu_probe): 0 = by density (default), 5 = word-parallel, 6 = word-parallel over head records, 1-4 list-based
     wait_timeout_us: int = 0     # bound of device-side waits; 0 = 10 s
     test_absent_block: int = 0   # failure-detection test hook (xbfs_opts.test_absent_block)
     _keep: list = field(default_factory=list, repr=False)

@@ -41,7 +41,37 @@ __global__ void k_adj_keys(const long long* __restrict__ beg, const int* __restr
   }
 }
 
+// Head record of every vertex (one thread each): its first three neighbours
+// in CSR order, -1 past its degree, and its degree (saturated at
+// kHeadDegSat). A bottom-up probe reads the 16-byte record, coalesced across
+// the 32 vertices of a bitmap word, instead of the vertex's CSR offsets and
+// then the first sector of its segment.
+__global__ void k_head(const long long* __restrict__ beg, const int* __restrict__ csr, long long V,
+                       int4* __restrict__ head) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x) {
+    const long long b0 = beg[v], d = beg[v + 1] - b0;
+    int4 h;
+    h.x = d > 0 ? csr[b0] : -1;
+    h.y = d > 1 ? csr[b0 + 1] : -1;
+    h.z = d > 2 ? csr[b0 + 2] : -1;
+    h.w = d < kHeadDegSat ? (int)d : kHeadDegSat;
+    head[v] = h;
+  }
+}
+
 }  // namespace
+
+xbfs_status graph_build_head(Graph* g) {
+  DeviceGuard dg(g->device);
+  xbfs_status st = g->head.ensure((size_t)g->V * sizeof(int4));
+  if (st) return st;
+  int nsm = 0;
+  XBFS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device));
+  k_head<<<nsm * 8, 256, 0, g->stream>>>(g->beg.as<long long>(), g->csr.as<int>(), g->V, g->head.as<int4>());
+  XBFS_CUDA_TRY(cudaGetLastError());
+  XBFS_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  return XBFS_OK;
+}
 
 xbfs_status graph_sort_adjacency(Graph* g, int order) {
   if (!g) return set_error(XBFS_ERR_INVALID_ARG, "graph is NULL");
@@ -71,7 +101,7 @@ xbfs_status graph_sort_adjacency(Graph* g, int order) {
     XBFS_CUDA_TRY(cudaMemcpyAsync(g->csr.p, vals.Current(), E * 4, cudaMemcpyDeviceToDevice, s));
   XBFS_CUDA_TRY(cudaStreamSynchronize(s));
   g->adj_order = order;
-  return XBFS_OK;
+  return graph_build_head(g);
 }
 
 }  // namespace xbfs

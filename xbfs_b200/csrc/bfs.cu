@@ -126,6 +126,7 @@ struct QBin {
 struct Params {
   const long long* beg;
   const int* csr;
+  const int4* head;  // per-vertex head records (first three neighbours, degree); null: CSR offsets only
   long long V, E;
   int* levels;
   int* parents;
@@ -1130,7 +1131,33 @@ __device__ __forceinline__ void bu_publish_words(const Params& p, uint32_t* fbn,
 // 32 vertices at a time from a shared counter, so a slow warp does not hold the
 // others. Each lane probes its vertex's neighbours 2, then 4, then 8 at a time
 // (most vertices find a parent among the first few).
-template <bool PAR, bool ASYNC>
+// Frontier probe of the three neighbours in a head record (-1 entries are
+// absent neighbours): a level-L parent, else with ASYNC the first of them
+// already in frontier L+1.
+template <bool ASYNC>
+__device__ __forceinline__ void probe_head(const uint32_t* fbc, const uint32_t* fbn, const int4& h, int& found,
+                                           int& found2) {
+  const int u[3] = {h.x, h.y, h.z};
+  uint32_t wc[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) wc[j] = u[j] >= 0 ? fbc[u[j] >> 5] : 0u;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    if (found < 0 && u[j] >= 0 && ((wc[j] >> (u[j] & 31)) & 1u)) found = u[j];
+  if (ASYNC && found < 0 && found2 < 0) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      if (found2 < 0 && u[j] >= 0 && ((ld_cg_u32(fbn + (u[j] >> 5)) >> (u[j] & 31)) & 1u)) found2 = u[j];
+  }
+}
+
+// Degree of v from its head record; a saturated field falls back to the CSR
+// offsets.
+__device__ __forceinline__ long long head_degree(const Params& p, const int4& h, int v) {
+  return h.w != kHeadDegSat ? (long long)h.w : ld_nc_i64(p.beg + v + 1) - ld_nc_i64(p.beg + v);
+}
+
+template <bool PAR, bool ASYNC, bool HEAD>
 __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
                           uint32_t* fbn2, const QOut& q2, bool asyncq) {
   const long long nw = p.nwords;
@@ -1221,7 +1248,40 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
     uint32_t word = 0xffffffffu, m1 = 0, m2 = 0;  // bitmap word of this lane's vertex, bits to set
     int v = -1;
     long long e0 = 0, e1 = 0;
-    if (i < n) {
+    if (i < n && HEAD) {
+      // head record first: three neighbours and the degree in one read;
+      // the CSR offsets only when the scan goes on (or a queue entry for
+      // frontier L+2 needs the vertex's offset)
+      v = list[i];
+      const int4 h = ld_nc_na_v4(p.head + v);
+      int found = -1, found2 = -1;
+      probe_head<ASYNC>(fbc, fbn, h, found, found2);
+      const long long d = head_degree(p, h, v);
+      if (found < 0 && d > 3) {
+        e0 = ld_nc_i64(p.beg + v);
+        long long e = e0 + 3;
+        probe_range<4, true, ASYNC>(p, fbc, fbn, e, e0 + 7 < e0 + d ? e0 + 7 : e0 + d, found, found2);
+        if (found < 0) probe_range<8, true, ASYNC>(p, fbc, fbn, e, e0 + d, found, found2);
+      } else if (ASYNC && asyncq && found < 0 && found2 >= 0) {
+        e0 = ld_nc_i64(p.beg + v);
+      }
+      e1 = e0 + d;
+      word = (uint32_t)v >> 5;
+      const uint32_t bit = 1u << (v & 31);
+      if (found >= 0) {
+        p.levels[v] = L + 1;
+        if (PAR) p.parents[v] = found;
+        m1 = bit;
+        acc.n1 += 1;
+        acc.m1 += d;
+      } else if (ASYNC && found2 >= 0) {
+        p.levels[v] = L + 2;
+        if (PAR) p.parents[v] = found2;
+        m2 = bit;
+        acc.n2 += 1;
+        acc.m2 += d;
+      }
+    } else if (i < n) {
       v = list[i];
       e0 = ld_nc_i64(p.beg + v);
       e1 = ld_nc_i64(p.beg + v + 1);
@@ -1278,6 +1338,70 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
   }
 }
 
+// Shape of the word-parallel bottom-up step (below): bitmap words per warp
+// step, neighbours probed before a vertex is deferred, neighbours per drain
+// step, capacity of the per-CTA deferred queue.
+#ifndef XBFS_BU_WORDS
+#define XBFS_BU_WORDS 2
+#endif
+#ifndef XBFS_BU_FIRST
+#define XBFS_BU_FIRST 2
+#endif
+constexpr int kBuWords = XBFS_BU_WORDS, kBuFirst = XBFS_BU_FIRST, kBuMore = 8;
+constexpr int kBuQueue = 2 * kCap;
+// Bottom-up probes read head records where the graph has them (1), or the
+// CSR offsets only (0); the word-parallel step over head records loads the
+// visited words of the warp's next step one step ahead (1) or not (0).
+#ifndef XBFS_BU_HEADS
+#define XBFS_BU_HEADS 1
+#endif
+#ifndef XBFS_BU_PREFETCH
+#define XBFS_BU_PREFETCH 1
+#endif
+constexpr bool kBuPrefetch = XBFS_BU_PREFETCH;
+
+// Second phase of the word-parallel bottom-up step: the vertices deferred to
+// the CTA's shared-memory queue (their first `first` neighbours probed
+// without a hit) are scanned one per lane, kBuMore neighbours per step.
+template <bool PAR, bool ASYNC>
+__device__ void bu_drain(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
+                         uint32_t* fbn2, int first) {
+  const int lane = threadIdx.x & 31;
+  const int* q_v = &sm.st_id[0][0];
+  const int nq = sm.bu_n < kBuQueue ? sm.bu_n : kBuQueue;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&sm.bu_next, 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= nq) break;
+    const int i = base + lane;
+    uint32_t word = 0xffffffffu, m1 = 0, m2 = 0;
+    if (i < nq) {
+      const int v = q_v[i];
+      const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
+      long long e = e0 + first;
+      int found = -1, found2 = -1;
+      probe_range<kBuMore, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+      word = (uint32_t)v >> 5;
+      const uint32_t bit = 1u << (v & 31);
+      if (found >= 0) {
+        p.levels[v] = L + 1;
+        if (PAR) p.parents[v] = found;
+        m1 = bit;
+        acc.n1 += 1;
+        acc.m1 += e1 - e0;
+      } else if (ASYNC && found2 >= 0) {
+        p.levels[v] = L + 2;
+        if (PAR) p.parents[v] = found2;
+        m2 = bit;
+        acc.n2 += 1;
+        acc.m2 += e1 - e0;
+      }
+    }
+    bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, m2, i < nq);
+  }
+}
+
 // Bottom-up step for level L, word-parallel (the default probe mode). Each
 // warp takes kBuWords consecutive words of its CTA's slice of the visited
 // bitmap at a time; lane i handles vertex 32w+i of each word when it is
@@ -1292,14 +1416,6 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
 // areas, unused in a bottom-up level) and drained afterwards one vertex per
 // lane, kBuMore neighbours per step, so a long scan no longer holds the 31
 // other lanes of its warp.
-#ifndef XBFS_BU_WORDS
-#define XBFS_BU_WORDS 2
-#endif
-#ifndef XBFS_BU_FIRST
-#define XBFS_BU_FIRST 2
-#endif
-constexpr int kBuWords = XBFS_BU_WORDS, kBuFirst = XBFS_BU_FIRST, kBuMore = 8;
-constexpr int kBuQueue = 2 * kCap;
 
 template <bool PAR, bool ASYNC>
 __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
@@ -1309,8 +1425,7 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NWARP = kBlock / 32;
-  int* q_v = &sm.st_id[0][0];        // deferred vertex
-  long long* q_e = &sm.st_bg[0][0];  // its next neighbour to probe
+  int* q_v = &sm.st_id[0][0];  // deferred vertices
   if (threadIdx.x == 0) {
     sm.bu_n = 0;
     sm.bu_next = 0;
@@ -1361,7 +1476,6 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
           const int slot = base + __popc(dm & ((1u << lane) - 1u));
           if (slot < kBuQueue) {
             q_v[slot] = (int)((wb + k) * 32 + lane);
-            q_e[slot] = e[k] + kBuFirst;
           } else {
             long long ex = e[k] + kBuFirst;
             probe_range<kBuMore, true, ASYNC>(p, fbc, fbn, ex, ee[k], found, found2);
@@ -1402,38 +1516,118 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
     }
   }
   __syncthreads();
-  const int nq = sm.bu_n < kBuQueue ? sm.bu_n : kBuQueue;
-  for (;;) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(&sm.bu_next, 32);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= nq) break;
-    const int i = base + lane;
-    uint32_t word = 0xffffffffu, m1 = 0, m2 = 0;
-    if (i < nq) {
-      const int v = q_v[i];
-      long long e = q_e[i];
-      const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
-      int found = -1, found2 = -1;
-      probe_range<kBuMore, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
-      word = (uint32_t)v >> 5;
-      const uint32_t bit = 1u << (v & 31);
-      if (found >= 0) {
-        p.levels[v] = L + 1;
-        if (PAR) p.parents[v] = found;
-        m1 = bit;
-        acc.n1 += 1;
-        acc.m1 += e1 - e0;
-      } else if (ASYNC && found2 >= 0) {
-        p.levels[v] = L + 2;
-        if (PAR) p.parents[v] = found2;
-        m2 = bit;
-        acc.n2 += 1;
-        acc.m2 += e1 - e0;
+  bu_drain<PAR, ASYNC>(p, sm, acc, L, fbc, fbn, fbn2, kBuFirst);
+}
+
+// Word-parallel bottom-up step over head records: the same work split and
+// deferred queue as bottom_up_words, but a lane reads its vertex's 16-byte
+// head record (first three neighbours and degree; the 32 records of a word
+// are one coalesced 512-byte read) in place of its CSR offsets followed by
+// the first CSR sector, and the visited words of the warp's next step are
+// loaded one step ahead. A probe is then two dependent reads (record, then
+// frontier bits) instead of four.
+template <bool PAR, bool ASYNC>
+__device__ void bottom_up_heads(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
+                                uint32_t* fbn2) {
+  constexpr int F = 3;  // neighbours in a head record
+  const long long nw = p.nwords;
+  const long long G = gridDim.x, b = blockIdx.x;
+  const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NWARP = kBlock / 32;
+  constexpr long long kStride = (long long)NWARP * kBuWords;
+  int* q_v = &sm.st_id[0][0];  // deferred vertices
+  if (threadIdx.x == 0) {
+    sm.bu_n = 0;
+    sm.bu_next = 0;
+  }
+  __syncthreads();
+  uint32_t un_nx[kBuWords];
+  if (kBuPrefetch) {
+    const long long wb = w0 + (long long)warp * kBuWords;
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k) un_nx[k] = (wb + k < w1) ? ~ld_cg_u32(p.vis + wb + k) : 0u;
+  }
+  for (long long wb = w0 + (long long)warp * kBuWords; wb < w1; wb += kStride) {
+    uint32_t un[kBuWords];
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k) {
+      if (kBuPrefetch) {
+        un[k] = un_nx[k];
+        un_nx[k] = (wb + kStride + k < w1) ? ~ld_cg_u32(p.vis + wb + kStride + k) : 0u;
+      } else {
+        un[k] = (wb + k < w1) ? ~ld_cg_u32(p.vis + wb + k) : 0u;
       }
     }
-    bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, m2, i < nq);
+    int4 h[kBuWords];
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k)
+      h[k] = ((un[k] >> lane) & 1u) ? ld_nc_na_v4(p.head + (wb + k) * 32 + lane) : make_int4(-1, -1, -1, 0);
+    uint32_t wc[kBuWords][F];
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k) {
+      wc[k][0] = h[k].x >= 0 ? fbc[h[k].x >> 5] : 0u;
+      wc[k][1] = h[k].y >= 0 ? fbc[h[k].y >> 5] : 0u;
+      wc[k][2] = h[k].z >= 0 ? fbc[h[k].z >> 5] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k) {
+      const bool act = (un[k] >> lane) & 1u;
+      const int v = (int)((wb + k) * 32 + lane);
+      const int u[F] = {h[k].x, h[k].y, h[k].z};
+      int found = -1, found2 = -1;
+#pragma unroll
+      for (int j = 0; j < F; ++j)
+        if (found < 0 && u[j] >= 0 && ((wc[k][j] >> (u[j] & 31)) & 1u)) found = u[j];
+      const long long d = act ? head_degree(p, h[k], v) : 0;
+      bool defer = act && found < 0 && d > F;
+      const unsigned dm = __ballot_sync(0xffffffffu, defer);
+      if (dm) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&sm.bu_n, __popc(dm));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (defer) {
+          const int slot = base + __popc(dm & ((1u << lane) - 1u));
+          if (slot < kBuQueue) {
+            q_v[slot] = v;
+          } else {
+            const long long e0 = ld_nc_i64(p.beg + v);
+            long long ex = e0 + F;
+            probe_range<kBuMore, true, ASYNC>(p, fbc, fbn, ex, e0 + d, found, found2);
+            defer = false;
+          }
+        }
+      }
+      if (ASYNC && act && found < 0 && !defer && found2 < 0) {
+#pragma unroll
+        for (int j = 0; j < F; ++j)
+          if (found2 < 0 && u[j] >= 0 && ((ld_cg_u32(fbn + (u[j] >> 5)) >> (u[j] & 31)) & 1u)) found2 = u[j];
+      }
+      const bool got1 = act && found >= 0;
+      const bool got2 = ASYNC && act && !got1 && !defer && found2 >= 0;
+      if (got1) {
+        p.levels[v] = L + 1;
+        if (PAR) p.parents[v] = found;
+        acc.n1 += 1;
+        acc.m1 += d;
+      } else if (got2) {
+        p.levels[v] = L + 2;
+        if (PAR) p.parents[v] = found2;
+        acc.n2 += 1;
+        acc.m2 += d;
+      }
+      const uint32_t m1 = __ballot_sync(0xffffffffu, got1);
+      const uint32_t m2 = __ballot_sync(0xffffffffu, got2);
+      if (lane == 0 && (m1 | m2)) {
+        const long long w = wb + k;
+        red_or_u32(p.vis + w, m1 | m2);
+        if (m1) red_or_u32(fbn + w, m1);
+        if (ASYNC && m2) red_or_u32(fbn2 + w, m2);
+      }
+    }
   }
+  __syncthreads();
+  bu_drain<PAR, ASYNC>(p, sm, acc, L, fbc, fbn, fbn2, F);
 }
 
 // Block-reduce the accumulators and publish them to the frontier descriptors.
@@ -1782,7 +1976,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       // bottom-up level of a power-law graph), else over the compacted list
       // of unvisited vertices (few per bitmap word: most lanes of a word
       // would idle)
-      const bool words = p.bu_mode == 5 || (p.bu_mode == 0 && sm.bu_dense);
+      const bool words = p.bu_mode >= 5 || (p.bu_mode == 0 && sm.bu_dense);
+      // head records, where the graph has them, in the default mode (and
+      // mode 6, word-parallel over head records only)
+      const bool heads = XBFS_BU_HEADS && p.head != nullptr && (p.bu_mode == 0 || p.bu_mode == 6);
       // on a sparse bottom-up level (list probing, few unvisited vertices)
       // the level-(L+2) winners of the asynchronous rule also go into
       // frontier L+2's queue, warp-aggregated (its counters are not used by
@@ -1793,15 +1990,25 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       qo2.ctr = F2->bin;
       const bool asyncq = XBFS_ASYNC_QUEUE && p.async_bu && !words && sm.asyncq_ok;
       if (threadIdx.x == 0 && asyncq) ls.pend_q_for = L + 2;
-      if (words) {
+      if (words && heads) {
+        if (p.async_bu)
+          bottom_up_heads<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+        else
+          bottom_up_heads<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
+      } else if (words) {
         if (p.async_bu)
           bottom_up_words<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
         else
           bottom_up_words<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
       } else if (p.async_bu) {
-        bottom_up<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2, qo2, asyncq);
+        if (heads)
+          bottom_up<PAR, true, true>(p, sm, acc, (int)L, fbc, fbn, fbn2, qo2, asyncq);
+        else
+          bottom_up<PAR, true, false>(p, sm, acc, (int)L, fbc, fbn, fbn2, qo2, asyncq);
+      } else if (heads) {
+        bottom_up<PAR, false, true>(p, sm, acc, (int)L, fbc, fbn, fbn2, qo2, false);
       } else {
-        bottom_up<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2, qo2, false);
+        bottom_up<PAR, false, false>(p, sm, acc, (int)L, fbc, fbn, fbn2, qo2, false);
       }
       publish_acc(sm, acc, F1, F2);
       if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
@@ -1901,6 +2108,7 @@ static xbfs_status setup_params(Graph* g, const xbfs_opts& o, int* d_levels, int
   SsWorkspace& w = g->ss;
   memset(&p, 0, sizeof(p));
   p.beg = g->beg.as<long long>();
+  p.head = g->head.as<int4>();
   p.csr = g->csr.as<int>();
   p.V = g->V;
   p.E = g->E;
@@ -2009,6 +2217,7 @@ xbfs_status bfs_single(Graph* g, int32_t src, int32_t* levels, int32_t* parents,
   if (o.policy == XBFS_POLICY_FORCED && (!o.forced || o.n_forced <= 0))
     return set_error(XBFS_ERR_INVALID_ARG, "forced policy needs a non-empty forced[] array");
   if (o.policy < 0 || o.policy > 3) return set_error(XBFS_ERR_INVALID_ARG, "bad policy %d", o.policy);
+  if (o.bu_probe < 0 || o.bu_probe > 6) return set_error(XBFS_ERR_INVALID_ARG, "bad bu_probe %d", o.bu_probe);
   if (!(o.alpha > 0)) o.alpha = 0.1f;
 
   DeviceGuard dg(g->device);
@@ -2126,6 +2335,7 @@ xbfs_status bfs_many(Graph* g, const int32_t* srcs, int32_t n, int32_t* levels, 
   if (o.policy == XBFS_POLICY_FORCED && (!o.forced || o.n_forced <= 0))
     return set_error(XBFS_ERR_INVALID_ARG, "forced policy needs a non-empty forced[] array");
   if (o.policy < 0 || o.policy > 3) return set_error(XBFS_ERR_INVALID_ARG, "bad policy %d", o.policy);
+  if (o.bu_probe < 0 || o.bu_probe > 6) return set_error(XBFS_ERR_INVALID_ARG, "bad bu_probe %d", o.bu_probe);
   if (o.small_max <= 0) o.small_max = 32;
   if (o.medium_max < o.small_max) o.medium_max = o.small_max;
   if (!(o.alpha > 0)) o.alpha = 0.1f;
@@ -2504,6 +2714,7 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
   if (o.policy == XBFS_POLICY_FORCED && (!o.forced || o.n_forced <= 0))
     return set_error(XBFS_ERR_INVALID_ARG, "forced policy needs a non-empty forced[] array");
   if (o.policy < 0 || o.policy > 3) return set_error(XBFS_ERR_INVALID_ARG, "bad policy %d", o.policy);
+  if (o.bu_probe < 0 || o.bu_probe > 6) return set_error(XBFS_ERR_INVALID_ARG, "bad bu_probe %d", o.bu_probe);
   if (!(o.alpha > 0)) o.alpha = 0.1f;
 
   DeviceGuard dg(g->device);
@@ -2561,6 +2772,7 @@ xbfs_status bfs_noalloc(Graph* g, int32_t src, int32_t* levels, int32_t* parents
   Params p;
   memset(&p, 0, sizeof(p));
   p.beg = g->beg.as<long long>();
+  p.head = g->head.as<int4>();
   p.csr = g->csr.as<int>();
   p.V = g->V;
   p.E = g->E;

@@ -73,6 +73,15 @@ __device__ __forceinline__ int ld_stream_i32(const int* p) {
       : "l"(p), "l"(l2_policy_evict_first()));
   return v;
 }
+// 16-byte read of data that is immutable during the launch, not kept in L1
+// (read once per level: L1 stays for the bitmap words probed at random).
+__device__ __forceinline__ int4 ld_nc_na_v4(const int4* p) {
+  int4 v;
+  asm("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(p));
+  return v;
+}
 __device__ __forceinline__ long long ld_nc_i64(const long long* p) {
   long long v;
   asm volatile("ld.global.nc.b64 %0, [%1];" : "=l"(v) : "l"(p));

@@ -246,7 +246,7 @@ xbfs_status graph_finish_upload(Graph* g) {
   g->max_degree = (int64_t)res.max_degree;
   g->n_isolated = (int64_t)res.n_isolated;
   for (int k = 0; k < 16; ++k) g->cnt_deg_gt[k] = (int64_t)res.cnt_deg_gt[k];
-  return XBFS_OK;
+  return graph_build_head(g);
 }
 
 xbfs_status validate_csr(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E) {

@@ -89,6 +89,7 @@ struct Graph {
   DevBuf beg;                    // int64[V+1]
   DevBuf csr;                    // int32[E] (+16 bytes tail padding)
   DevBuf iso;                    // uint32 bitmap: isolated vertices + tail bits
+  DevBuf head;                   // int4[V]: first three neighbours (-1 past the degree), degree
   cudaStream_t stream = nullptr;
   SsWorkspace ss;
   ~Graph();
@@ -107,7 +108,11 @@ struct DeviceGuard {
 };
 
 // graph.cpp
-xbfs_status graph_finish_upload(Graph* g);  // degree stats, iso bitmap, stream
+xbfs_status graph_finish_upload(Graph* g);  // degree stats, iso bitmap, stream, head records
+// adjacency.cu: (re)writes g->head from the current neighbour order
+xbfs_status graph_build_head(Graph* g);
+// Degree field of a head record saturates here; the CSR offsets give the rest.
+constexpr int kHeadDegSat = 0x7fffffff;
 xbfs_status graph_from_host(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E,
                             int device, bool validate, Graph** out);
 xbfs_status validate_csr(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E);
