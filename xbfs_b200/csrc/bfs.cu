@@ -540,24 +540,24 @@ __device__ __forceinline__ void claim_td(const Params& p, Smem& sm, const QOut& 
 // overlap, and the offsets are read for winners only: on a level where many
 // edges race for the same fresh targets, reading them for every candidate
 // (claim_td's speculative order) costs a random DRAM sector per losing edge.
-template <bool PAR>
-__device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int (&v)[kTdIlp], const int (&u)[kTdIlp],
-                                            int L, uint32_t* fbn, const QOut& q, bool qside) {
-  uint32_t vw[kTdIlp];
+template <bool PAR, int N>
+__device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int (&v)[N], const int (&u)[N], int L,
+                                            uint32_t* fbn, const QOut& q, bool qside) {
+  uint32_t vw[N];
 #pragma unroll
-  for (int k = 0; k < kTdIlp; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
-  bool win[kTdIlp];
+  for (int k = 0; k < N; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
+  bool win[N];
 #pragma unroll
-  for (int k = 0; k < kTdIlp; ++k) {
+  for (int k = 0; k < N; ++k) {
     win[k] = false;
     if (v[k] >= 0 && !((vw[k] >> (v[k] & 31)) & 1u)) {
       const uint32_t bit = 1u << (v[k] & 31);
       win[k] = (atomicOr(p.vis + (v[k] >> 5), bit) & bit) == 0;
     }
   }
-  long long b0[kTdIlp], d[kTdIlp];
+  long long b0[N], d[N];
 #pragma unroll
-  for (int k = 0; k < kTdIlp; ++k) {
+  for (int k = 0; k < N; ++k) {
     b0[k] = 0;
     d[k] = 0;
     if (!win[k]) continue;
@@ -568,7 +568,7 @@ __device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int
     d[k] = ld_nc_i64(p.beg + v[k] + 1) - b0[k];
   }
 #pragma unroll
-  for (int k = 0; k < kTdIlp; ++k)
+  for (int k = 0; k < N; ++k)
     if (win[k]) {
       acc.n1 += 1;
       acc.m1 += d[k];
@@ -611,12 +611,73 @@ __device__ __forceinline__ int smem_owner(const unsigned* web, int n, unsigned l
   return a;
 }
 
+// Bins with bitmap output are expanded by gather_bin_warp (1) or in
+// gather_bin's block rounds (0).
+#ifndef XBFS_TD_WARP_GATHER
+#define XBFS_TD_WARP_GATHER 1
+#endif
+
+// Edge-balanced expansion of a bin (or the heavy list) with bitmap output,
+// barrier-free: the CTA's share of the bin's edges is split evenly between
+// its warps, and each warp walks its range with the 32 bin entries that own
+// the next edges held one per lane (vertex, CSR offset, first edge), kTdIlp
+// edges per lane in flight; an edge's owner is found by a search over the
+// lanes. The entries are reloaded only when the range passes the 32nd.
+template <bool PAR>
+__device__ void gather_bin_warp(const Params& p, Acc& acc, const QOut& q, const QBin& in, unsigned cnt,
+                                unsigned long long M, int L, uint32_t* fbn, bool qside) {
+  if (cnt == 0 || M == 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NWARP = kBlock / 32;
+  const unsigned long long NW = (unsigned long long)gridDim.x * NWARP, gw = (unsigned long long)blockIdx.x * NWARP + warp;
+  const unsigned long long lo = M * gw / NW, hi = M * (gw + 1) / NW;
+  if (lo >= hi) return;
+  unsigned s = (unsigned)find_owner(in.eb, cnt, lo);
+  for (unsigned long long r = lo; r < hi;) {
+    // entries s .. s + 31, one per lane, and the first edge past them
+    const unsigned slot = s + (unsigned)lane;
+    const unsigned eb = slot < cnt ? in.eb[slot] : 0xffffffffu;
+    const int id = slot < cnt ? in.ids[slot] : 0;
+    const long long bg = slot < cnt ? in.bg[slot] : 0;
+    unsigned long long wend = M;
+    if (lane == 31 && slot + 1 < cnt) wend = in.eb[slot + 1];
+    wend = __shfl_sync(0xffffffffu, wend, 31);
+    const unsigned long long rend = wend < hi ? wend : hi;
+    for (; r < rend; r += 32 * kTdIlp) {
+      int v[kTdIlp], u[kTdIlp];
+#pragma unroll
+      for (int k = 0; k < kTdIlp; ++k) {
+        const unsigned long long e = r + 32 * k + lane;
+        int o = 0;  // last lane whose entry starts at or before e
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1) {
+          const unsigned x = __shfl_sync(0xffffffffu, eb, o + st);
+          if ((unsigned long long)x <= e) o += st;
+        }
+        const unsigned xo = __shfl_sync(0xffffffffu, eb, o);
+        const long long bo = __shfl_sync(0xffffffffu, bg, o);
+        u[k] = __shfl_sync(0xffffffffu, id, o);
+        v[k] = e < rend ? ld_stream_i32(p.csr + bo + (long long)(e - xo)) : -1;
+      }
+      claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
+    }
+    if (rend < hi) {
+      r = rend;
+      s += 32;
+    }
+  }
+}
+
 // Edge-balanced expansion of one bin of the current frontier queue (medium
 // and large bins, and the heavy list of a fused sweep).
 template <bool PAR>
 __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
                            unsigned long long M, int L, bool enq, uint32_t* fbn, bool qside) {
   if (cnt == 0 || M == 0) return;
+  if (!enq && XBFS_TD_WARP_GATHER) {
+    gather_bin_warp<PAR>(p, acc, q, in, cnt, M, L, fbn, qside);
+    return;
+  }
   const bool spec = sm.spec != 0;
   const unsigned long long G = gridDim.x, b = blockIdx.x;
   const unsigned long long lo = M * b / G, hi = M * (b + 1) / G;
@@ -866,6 +927,134 @@ __device__ void gather_entries_warp(const Params& p, const QOut& q, const QBin& 
   if (lane == 0) {
     if (n1) atomicAdd(&f1->n, (unsigned long long)n1);
     if (m1) atomicAdd(&f1->m, (unsigned long long)m1);
+  }
+}
+
+// Degree of v from its head record; a saturated field falls back to the CSR
+// offsets.
+__device__ __forceinline__ long long head_degree(const Params& p, const int4& h, int v) {
+  return h.w != kHeadDegSat ? (long long)h.w : ld_nc_i64(p.beg + v + 1) - ld_nc_i64(p.beg + v);
+}
+
+// Position of the k-th (0-based) set bit of m; m has more than k set bits.
+__device__ __forceinline__ int nth_set_bit(uint32_t m, int k) {
+  int pos = 0;  // largest pos with popc(m below pos) <= k
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1)
+    if (__popc(m & ((1u << (pos + s)) - 1u)) <= k) pos += s;
+  return pos;
+}
+
+// Last lane l of the warp with ex[l] <= t (ex non-decreasing over the lanes,
+// ex[0] = 0 <= t): the lane whose range [ex[l], ex[l] + count[l]) holds t.
+// Branch-free, every lane takes part in every shuffle.
+__device__ __forceinline__ int lane_owner(int ex, int t) {
+  int lo = 0;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const int exc = __shfl_sync(0xffffffffu, ex, lo + s);
+    if (exc <= t) lo += s;
+  }
+  return lo;
+}
+
+// Top-down from a frontier held only as a bitmap, with bitmap output, over
+// head records, with no block barrier: each warp takes 32 words of its CTA's
+// slice at a time (one per lane), numbers their set bits with a warp scan
+// and takes the frontier vertices 64 at a time, two per lane. A lane reads
+// its vertices' head records and claims the (up to) three neighbours in
+// them; the rest of each segment (from the fourth neighbour) is expanded by
+// the warp edge-balanced over its 32 lanes, kTdIlp edges per lane in flight.
+// Segments with more than kWarpSeg edges left go to the heavy list that is
+// expanded grid-wide, edge-balanced, after the barrier (as expand_bitmap's
+// vertices of degree above kHeavyDeg): warps do not wait for one another,
+// and no warp is held up by a long segment.
+#ifndef XBFS_TD_WARP_SEG
+#define XBFS_TD_WARP_SEG 1024
+#endif
+constexpr int kWarpSeg = XBFS_TD_WARP_SEG;
+template <bool PAR>
+__device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const QOut& q, const uint32_t* fbc, int L,
+                                    uint32_t* fbn, int par, bool qside) {
+  const long long nw = p.nwords;
+  const long long G = gridDim.x, b = blockIdx.x;
+  const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NWARP = kBlock / 32;
+  unsigned long long* hctr = &p.ctl->heavy[par];
+  // the warp's 64 vertices and their segments' next CSR offsets, for the
+  // edge-balanced expansion (the window arrays are free in this mode)
+  int* wu = sm.wu + warp * 64;
+  long long* wbg = sm.wbeg + warp * 64;
+  for (long long c = w0 + (long long)warp * 32; c < w1; c += (long long)NWARP * 32) {
+    const uint32_t bits = (c + lane < w1) ? ld_cg_u32(fbc + c + lane) : 0u;
+    const int pc = __popc(bits);
+    const int incl = warp_inclusive_scan(pc);
+    const int ex = incl - pc;
+    const int B = __shfl_sync(0xffffffffu, incl, 31);
+    for (int base = 0; base < B; base += 64) {
+      int uu[2];
+      int4 h[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int t = base + 32 * j + lane;
+        const int lo = lane_owner(ex, t);
+        const uint32_t wbits = __shfl_sync(0xffffffffu, bits, lo);
+        const int exl = __shfl_sync(0xffffffffu, ex, lo);
+        uu[j] = t < B ? (int)((c + lo) * 32 + nth_set_bit(wbits, t - exl)) : -1;
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) h[j] = uu[j] >= 0 ? ld_nc_na_v4(p.head + uu[j]) : make_int4(-1, -1, -1, 0);
+      // the segments' CSR offsets (where they go on past the head record)
+      // are loaded alongside the claims of the head neighbours
+      int r[2];
+      long long bg[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const long long rem = uu[j] >= 0 ? head_degree(p, h[j], uu[j]) - 3 : 0;
+        bg[j] = rem > 0 ? ld_nc_i64(p.beg + uu[j]) + 3 : 0;
+        r[j] = rem > kWarpSeg ? -1 : (rem > 0 ? (int)rem : 0);
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int v[3] = {h[j].x, h[j].y, h[j].z};
+        const int u[3] = {uu[j], uu[j], uu[j]};
+        claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        if (r[j] < 0) {
+          direct_enqueue(p.heavy, hctr, uu[j], head_degree(p, h[j], uu[j]) - 3, bg[j]);
+          r[j] = 0;
+        }
+        wu[32 * j + lane] = uu[j];
+        wbg[32 * j + lane] = bg[j];
+      }
+      __syncwarp();
+      // the rest of the 64 segments, edge-balanced over the warp: lane l
+      // owns edges [rex, rex + r[0] + r[1]) of the warp's total, its first
+      // vertex's r[0] and then its second vertex's r[1]
+      const int rr = r[0] + r[1];
+      const int rincl = warp_inclusive_scan(rr);
+      const int rex = rincl - rr;
+      const int T = __shfl_sync(0xffffffffu, rincl, 31);
+      for (int e0 = 0; e0 < T; e0 += 32 * kTdIlp) {
+        int v[kTdIlp], u[kTdIlp];
+#pragma unroll
+        for (int k = 0; k < kTdIlp; ++k) {
+          const int e = e0 + 32 * k + lane;
+          const int o = lane_owner(rex, e);
+          int off = e - __shfl_sync(0xffffffffu, rex, o);
+          const int r0 = __shfl_sync(0xffffffffu, r[0], o);
+          const int slot = off >= r0 ? 32 + o : o;
+          off = off >= r0 ? off - r0 : off;
+          u[k] = wu[slot];
+          v[k] = e < T ? __ldg(p.csr + wbg[slot] + off) : -1;
+        }
+        claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
+      }
+      __syncwarp();  // the next round rewrites the warp's entries
+    }
   }
 }
 
@@ -1151,12 +1340,6 @@ __device__ __forceinline__ void probe_head(const uint32_t* fbc, const uint32_t* 
   }
 }
 
-// Degree of v from its head record; a saturated field falls back to the CSR
-// offsets.
-__device__ __forceinline__ long long head_degree(const Params& p, const int4& h, int v) {
-  return h.w != kHeadDegSat ? (long long)h.w : ld_nc_i64(p.beg + v + 1) - ld_nc_i64(p.beg + v);
-}
-
 template <bool PAR, bool ASYNC, bool HEAD>
 __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
                           uint32_t* fbn2, const QOut& q2, bool asyncq) {
@@ -1354,6 +1537,11 @@ constexpr int kBuQueue = 2 * kCap;
 // visited words of the warp's next step one step ahead (1) or not (0).
 #ifndef XBFS_BU_HEADS
 #define XBFS_BU_HEADS 1
+#endif
+// Top-down levels from a frontier bitmap with bitmap output read head
+// records, barrier-free per warp (1), or take expand_bitmap's block tiles (0).
+#ifndef XBFS_TD_HEADS
+#define XBFS_TD_HEADS 1
 #endif
 #ifndef XBFS_BU_PREFETCH
 #define XBFS_BU_PREFETCH 1
@@ -1945,6 +2133,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
                             qside);
           }
           gather_entries<PAR>(p, sm, qo, acc, p.q[par][0], cnt0, pk0 >> 31, (int)L, enq, fbn, qside);
+        } else if (XBFS_TD_HEADS && !enq && p.head) {
+          expand_bitmap_heads<PAR>(p, sm, acc, qo, fbc, (int)L, fbn, par, qside);
         } else {
           expand_bitmap<PAR>(p, sm, qo, acc, fbc, (int)L, enq, fbn, par, qside);
         }
