@@ -241,6 +241,29 @@ def test_bottom_up_probe_modes(bu_mode):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("schedule", [["td_queue", "td_queue", "td_scan", "bu"],
+                                      ["td_queue", "td_scan", "td_scan", "td_scan"],
+                                      ["td_scan"]])
+def test_top_down_levels_with_many_fresh_targets(schedule):
+    """Top-down levels with bitmap output and many unvisited vertices mark
+    their targets and finalize them after a barrier (small-bin claims may
+    take some of them in the same level): levels equal the oracle's, parents
+    form a valid tree, on degree-ordered R-MAT (hub frontiers) and a grid."""
+    for beg, csr in (gen_rmat_host(17, 16, 5), gen_grid_host(300, 200)):
+        g = Graph.from_csr(beg, csr)
+        g.sort_adjacency("degree")
+        b2, c2 = g.download()
+        for s in pick_sources(b2, 3, 9):
+            ref = oracle.bfs_queue(b2, c2, int(s))
+            r = g.bfs(int(s), want_parents=True, policy="forced", forced=schedule)
+            assert np.array_equal(r.levels, ref), schedule
+            assert oracle.check_tree(b2, c2, int(s), r.levels, r.parents) == 0
+            r2 = g.bfs(int(s), policy="forced", forced=schedule)
+            assert np.array_equal(r2.levels, ref), schedule
+        g.free()
+
+
+@pytest.mark.gpu
 def test_bottom_up_probe_mode_out_of_range_is_refused():
     beg, csr = gen_rmat_host(10, 8, 2)
     g = Graph.from_csr(beg, csr)

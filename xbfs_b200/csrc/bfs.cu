@@ -76,6 +76,24 @@ constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: 
 #ifndef XBFS_ASYNC_QUEUE
 #define XBFS_ASYNC_QUEUE 1
 #endif
+// Top-down levels with bitmap output, many unvisited vertices and many
+// frontier edges run in two phases, marks then finalize_marks (1), or claim
+// their targets with returning atomics (0).
+#ifndef XBFS_TD_MARK
+#define XBFS_TD_MARK 1
+#endif
+// A mark first reads the target's word of frontier L+1's bitmap too and
+// skips the reduction when the bit is already there (1), or reduces
+// whenever the target is unvisited (0: one random read per edge fewer,
+// measured slightly faster on the hub levels of R-MAT scale 23).
+#ifndef XBFS_MARK_FBN_CHECK
+#define XBFS_MARK_FBN_CHECK 0
+#endif
+// Bins with bitmap output are expanded by gather_bin_warp (1) or in
+// gather_bin's block rounds (0).
+#ifndef XBFS_TD_WARP_GATHER
+#define XBFS_TD_WARP_GATHER 1
+#endif
 #ifndef XBFS_TD_ILP
 #define XBFS_TD_ILP 4
 #endif
@@ -213,6 +231,7 @@ struct __align__(16) Smem {
   int bu_next;
   int bu_n;
   int bu_dense;                 // this level's unvisited vertices are at least a quarter of V
+  int mark_ok;                  // many unvisited vertices and frontier edges: a bitmap-output level runs in two phases
   int qside_ok;                 // few unvisited vertices and every early next-frontier entry queued:
                                 // a top-down level with bitmap output also fills the next queue
   int asyncq_ok;                // a sparse bottom-up level: its asynchronous winners are queued
@@ -579,6 +598,35 @@ __device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int
     }
 }
 
+// Marking form of claim_batch for a top-down level with many fresh targets
+// (two-phase level): a target that is not visited (and, with
+// XBFS_MARK_FBN_CHECK, not yet in frontier L+1's bitmap) gets its bit there
+// by a reduction (no return value, so no thread waits on it), and with PAR
+// its parent is stored: every edge that
+// passes the test comes from frontier L, so whichever store lands last is a
+// valid parent. Nothing else is written; finalize_marks then turns the new
+// bits that no claim of the same level took (claims set the visited bit at
+// once) into levels, visited bits and frontier statistics. A target may
+// pass the test on several edges before the first reduction lands: its bit
+// is just set more than once.
+template <bool PAR, int N>
+__device__ __forceinline__ void mark_batch(const Params& p, const int (&v)[N], const int (&u)[N], uint32_t* fbn) {
+  uint32_t vw[N], fw[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
+    fw[k] = (XBFS_MARK_FBN_CHECK && v[k] >= 0) ? ld_cg_u32(fbn + (v[k] >> 5)) : 0u;
+  }
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    if (v[k] < 0) continue;
+    const uint32_t bit = 1u << (v[k] & 31);
+    if ((vw[k] | fw[k]) & bit) continue;
+    red_or_u32(fbn + (v[k] >> 5), bit);
+    if (PAR) p.parents[v[k]] = u[k];
+  }
+}
+
 // Warp-parallel search: last slot s in [0, cnt) with eb[s] <= key (eb strictly
 // increasing from eb[0] = 0 <= key). Called by a full warp.
 __device__ int find_owner(const unsigned* eb, unsigned cnt, unsigned long long key) {
@@ -611,12 +659,6 @@ __device__ __forceinline__ int smem_owner(const unsigned* web, int n, unsigned l
   return a;
 }
 
-// Bins with bitmap output are expanded by gather_bin_warp (1) or in
-// gather_bin's block rounds (0).
-#ifndef XBFS_TD_WARP_GATHER
-#define XBFS_TD_WARP_GATHER 1
-#endif
-
 // Edge-balanced expansion of a bin (or the heavy list) with bitmap output,
 // barrier-free: the CTA's share of the bin's edges is split evenly between
 // its warps, and each warp walks its range with the 32 bin entries that own
@@ -625,7 +667,7 @@ __device__ __forceinline__ int smem_owner(const unsigned* web, int n, unsigned l
 // lanes. The entries are reloaded only when the range passes the 32nd.
 template <bool PAR>
 __device__ void gather_bin_warp(const Params& p, Acc& acc, const QOut& q, const QBin& in, unsigned cnt,
-                                unsigned long long M, int L, uint32_t* fbn, bool qside) {
+                                unsigned long long M, int L, uint32_t* fbn, bool qside, bool mark) {
   if (cnt == 0 || M == 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NWARP = kBlock / 32;
@@ -659,7 +701,10 @@ __device__ void gather_bin_warp(const Params& p, Acc& acc, const QOut& q, const 
         u[k] = __shfl_sync(0xffffffffu, id, o);
         v[k] = e < rend ? ld_stream_i32(p.csr + bo + (long long)(e - xo)) : -1;
       }
-      claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
+      if (mark)
+        mark_batch<PAR>(p, v, u, fbn);
+      else
+        claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
     }
     if (rend < hi) {
       r = rend;
@@ -672,10 +717,10 @@ __device__ void gather_bin_warp(const Params& p, Acc& acc, const QOut& q, const 
 // and large bins, and the heavy list of a fused sweep).
 template <bool PAR>
 __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
-                           unsigned long long M, int L, bool enq, uint32_t* fbn, bool qside) {
+                           unsigned long long M, int L, bool enq, uint32_t* fbn, bool qside, bool mark = false) {
   if (cnt == 0 || M == 0) return;
-  if (!enq && XBFS_TD_WARP_GATHER) {
-    gather_bin_warp<PAR>(p, acc, q, in, cnt, M, L, fbn, qside);
+  if (!enq && (XBFS_TD_WARP_GATHER || mark)) {
+    gather_bin_warp<PAR>(p, acc, q, in, cnt, M, L, fbn, qside, mark);
     return;
   }
   const bool spec = sm.spec != 0;
@@ -975,7 +1020,7 @@ __device__ __forceinline__ int lane_owner(int ex, int t) {
 constexpr int kWarpSeg = XBFS_TD_WARP_SEG;
 template <bool PAR>
 __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const QOut& q, const uint32_t* fbc, int L,
-                                    uint32_t* fbn, int par, bool qside) {
+                                    uint32_t* fbn, int par, bool qside, bool mark) {
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
@@ -1019,7 +1064,10 @@ __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const Q
       for (int j = 0; j < 2; ++j) {
         const int v[3] = {h[j].x, h[j].y, h[j].z};
         const int u[3] = {uu[j], uu[j], uu[j]};
-        claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
+        if (mark)
+          mark_batch<PAR>(p, v, u, fbn);
+        else
+          claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
       }
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
@@ -1051,9 +1099,62 @@ __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const Q
           u[k] = wu[slot];
           v[k] = e < T ? __ldg(p.csr + wbg[slot] + off) : -1;
         }
-        claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
+        if (mark)
+          mark_batch<PAR>(p, v, u, fbn);
+        else
+          claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
       }
       __syncwarp();  // the next round rewrites the warp's entries
+    }
+  }
+}
+
+// Second phase of a two-phase top-down level (after a grid barrier, when
+// every mark has landed): the new vertices are the bits of frontier L+1's
+// bitmap that are not visited. Each warp takes 32 words of its CTA's slice
+// (one per lane), sets their visited bits (one thread per word), and then
+// takes the new vertices 64 at a time, two per lane: level L+1, and the
+// frontier statistics with the degrees from their head records.
+__device__ void finalize_marks(const Params& p, Acc& acc, int L, const uint32_t* fbn) {
+  const long long nw = p.nwords;
+  const long long G = gridDim.x, b = blockIdx.x;
+  const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NWARP = kBlock / 32;
+  for (long long c = w0 + (long long)warp * 32; c < w1; c += (long long)NWARP * 32) {
+    uint32_t nb = 0;
+    if (c + lane < w1) {
+      const uint32_t f = ld_cg_u32(fbn + c + lane);
+      if (f) {
+        const uint32_t vv = ld_cg_u32(p.vis + c + lane);
+        nb = f & ~vv;
+        if (nb) p.vis[c + lane] = vv | nb;
+      }
+    }
+    const int pc = __popc(nb);
+    const int incl = warp_inclusive_scan(pc);
+    const int ex = incl - pc;
+    const int B = __shfl_sync(0xffffffffu, incl, 31);
+    for (int base = 0; base < B; base += 64) {
+      int nv[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int t = base + 32 * j + lane;
+        const int lo = lane_owner(ex, t);
+        const uint32_t wbits = __shfl_sync(0xffffffffu, nb, lo);
+        const int exl = __shfl_sync(0xffffffffu, ex, lo);
+        nv[j] = t < B ? (int)((c + lo) * 32 + nth_set_bit(wbits, t - exl)) : -1;
+      }
+      int4 h[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) h[j] = nv[j] >= 0 ? ld_nc_na_v4(p.head + nv[j]) : make_int4(-1, -1, -1, 0);
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        if (nv[j] >= 0) {
+          p.levels[nv[j]] = L + 1;
+          acc.n1 += 1;
+          acc.m1 += head_degree(p, h[j], nv[j]);
+        }
     }
   }
 }
@@ -2025,6 +2126,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         if (m_u < 0) m_u = 0;
         sm.bu_dense = (n_u * 4 >= p.V) ? 1 : 0;
         sm.asyncq_ok = (n_u * 4 < p.V) ? 1 : 0;
+        sm.mark_ok = (n_u * 16 >= p.V && m_f * 2 >= p.V) ? 1 : 0;
         sm.qside_ok = (n_u * 64 <= p.V && (pn == 0 || ls.pend_q_for == L + 1)) ? 1 : 0;
         switch (p.policy) {
           case XBFS_POLICY_FORCED: {
@@ -2111,6 +2213,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       // so a small next level expands the queue instead of sweeping the
       // bitmap (the bitmap stays valid too)
       const bool qside = !enq && sm.qside_ok;
+      // A level with bitmap output and many unvisited vertices runs in two
+      // phases: marks of fresh targets into frontier L+1's bitmap without
+      // atomics that return (the bitmap sweep, the medium and large bins
+      // and the heavy list; the small bin still claims), then, after a
+      // barrier, finalize_marks: levels, visited bits and statistics of the
+      // marked vertices that no claim took
+      const bool mark = XBFS_TD_MARK && !enq && p.head && sm.mark_ok && !qside;
       QOut qo;
       for (int b2 = 0; b2 < 3; ++b2) qo.b[b2] = p.q[par ^ 1][b2];
       qo.ctr = F1->bin;
@@ -2130,11 +2239,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
           for (int bin = 2; bin >= 1; --bin) {
             const unsigned long long pk = sm.bins[bin];
             gather_bin<PAR>(p, sm, qo, acc, p.q[par][bin], (unsigned)(pk & kCountMask), pk >> 31, (int)L, enq, fbn,
-                            qside);
+                            qside, mark);
           }
           gather_entries<PAR>(p, sm, qo, acc, p.q[par][0], cnt0, pk0 >> 31, (int)L, enq, fbn, qside);
-        } else if (XBFS_TD_HEADS && !enq && p.head) {
-          expand_bitmap_heads<PAR>(p, sm, acc, qo, fbc, (int)L, fbn, par, qside);
+        } else if ((XBFS_TD_HEADS || mark) && !enq && p.head) {
+          expand_bitmap_heads<PAR>(p, sm, acc, qo, fbc, (int)L, fbn, par, qside, mark);
         } else {
           expand_bitmap<PAR>(p, sm, qo, acc, fbc, (int)L, enq, fbn, par, qside);
         }
@@ -2147,11 +2256,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         // (the list is complete only after the barrier; usually it is empty)
         const unsigned long long hk = ld_cg_u64(&ctl->heavy[par]);
         if ((hk & kCountMask) != 0) {
-          gather_bin<PAR>(p, sm, qo, acc, p.heavy, (unsigned)(hk & kCountMask), hk >> 31, (int)L, enq, fbn, qside);
+          gather_bin<PAR>(p, sm, qo, acc, p.heavy, (unsigned)(hk & kCountMask), hk >> 31, (int)L, enq, fbn, qside,
+                          mark);
           if (enq) flush(sm, qo);
           publish_acc(sm, acc, F1, nullptr);
           if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
         }
+      }
+      if (mark) {
+        finalize_marks(p, acc, (int)L, fbn);
+        publish_acc(sm, acc, F1, nullptr);
+        if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       }
       q_valid = enq || qside;
       b_valid = !enq;
