@@ -97,6 +97,11 @@ constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: 
 #ifndef XBFS_TD_ILP
 #define XBFS_TD_ILP 4
 #endif
+// Sparse (list-probing) bottom-up levels apply the asynchronous level-(L+2)
+// rule when async_bu is set (1) or never (0).
+#ifndef XBFS_BU_ASYNC_LIST
+#define XBFS_BU_ASYNC_LIST 1
+#endif
 constexpr int kTdIlp = XBFS_TD_ILP; // edges per thread in flight in the barrier-free top-down loops
 constexpr int kCap = 1024;          // staging capacity, small and medium bins
 constexpr int kCapL = 256;          // staging capacity, large bin
@@ -1648,16 +1653,29 @@ constexpr int kBuQueue = 2 * kCap;
 #define XBFS_BU_PREFETCH 1
 #endif
 constexpr bool kBuPrefetch = XBFS_BU_PREFETCH;
+// The word-parallel step over head records tests the vertices whose whole
+// list is in the record for level L+2 (asynchronous rule) (1) or leaves
+// them to the next level (0: one dependent read of frontier L+1's bitmap
+// fewer per step; the first bottom-up level of R-MAT scale 23 measured
+// 30-35% faster, the next level a little slower, the traversal 11%
+// faster). The drain of deferred vertices applies the rule (1) or not (0:
+// measured 1% faster; the list-probing levels keep the rule).
+#ifndef XBFS_BU_FOUND2
+#define XBFS_BU_FOUND2 0
+#endif
+#ifndef XBFS_BU_ASYNC_DRAIN
+#define XBFS_BU_ASYNC_DRAIN 0
+#endif
 
 // Second phase of the word-parallel bottom-up step: the vertices deferred to
 // the CTA's shared-memory queue (their first `first` neighbours probed
 // without a hit) are scanned one per lane, kBuMore neighbours per step.
 template <bool PAR, bool ASYNC>
 __device__ void bu_drain(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
-                         uint32_t* fbn2, int first) {
+                         uint32_t* fbn2, int first, const int* gq) {
   const int lane = threadIdx.x & 31;
   const int* q_v = &sm.st_id[0][0];
-  const int nq = sm.bu_n < kBuQueue ? sm.bu_n : kBuQueue;
+  const int nq = sm.bu_n;
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&sm.bu_next, 32);
@@ -1666,11 +1684,11 @@ __device__ void bu_drain(const Params& p, Smem& sm, Acc& acc, int L, const uint3
     const int i = base + lane;
     uint32_t word = 0xffffffffu, m1 = 0, m2 = 0;
     if (i < nq) {
-      const int v = q_v[i];
+      const int v = i < kBuQueue ? q_v[i] : gq[i - kBuQueue];
       const long long e0 = ld_nc_i64(p.beg + v), e1 = ld_nc_i64(p.beg + v + 1);
       long long e = e0 + first;
       int found = -1, found2 = -1;
-      probe_range<kBuMore, true, ASYNC>(p, fbc, fbn, e, e1, found, found2);
+      probe_range<kBuMore, true, ASYNC && XBFS_BU_ASYNC_DRAIN>(p, fbc, fbn, e, e1, found, found2);
       word = (uint32_t)v >> 5;
       const uint32_t bit = 1u << (v & 31);
       if (found >= 0) {
@@ -1701,10 +1719,11 @@ __device__ void bu_drain(const Params& p, Smem& sm, Acc& acc, int L, const uint3
 // is built (the bitmap word is the lanes' work), and results go out with
 // one atomic per word. On power-law graphs most unvisited vertices find a
 // parent within the first few neighbours; one that still has neighbours
-// left is deferred to a per-CTA queue in shared memory (the top-down staging
-// areas, unused in a bottom-up level) and drained afterwards one vertex per
-// lane, kBuMore neighbours per step, so a long scan no longer holds the 31
-// other lanes of its warp.
+// left is deferred to a per-CTA queue (in shared memory, the top-down
+// staging areas unused in a bottom-up level, and past kBuQueue entries in
+// the CTA's part of the bottom-up list area) and drained afterwards one
+// vertex per lane, kBuMore neighbours per step, so a long scan no longer
+// holds the 31 other lanes of its warp.
 
 template <bool PAR, bool ASYNC>
 __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, const uint32_t* fbc, uint32_t* fbn,
@@ -1714,7 +1733,8 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NWARP = kBlock / 32;
-  int* q_v = &sm.st_id[0][0];  // deferred vertices
+  int* q_v = &sm.st_id[0][0];  // deferred vertices, then (past kBuQueue) the slice's part of p.ulist
+  int* gq = p.ulist + w0 * 32;
   if (threadIdx.x == 0) {
     sm.bu_n = 0;
     sm.bu_next = 0;
@@ -1754,8 +1774,8 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
         if (found < 0 && u[k][j] >= 0 && ((wc[k][j] >> (u[k][j] & 31)) & 1u)) found = u[k][j];
       const long long d = ee[k] - e[k];
       bool defer = act && found < 0 && d > kBuFirst;
-      // warp-aggregated slots in the deferred queue; a full queue is not an
-      // error: the lane then scans the rest of its vertex here
+      // warp-aggregated slots in the deferred queue (shared memory first,
+      // then the CTA's part of the list area, which holds its whole slice)
       const unsigned dm = __ballot_sync(0xffffffffu, defer);
       if (dm) {
         int base = 0;
@@ -1763,13 +1783,10 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
         base = __shfl_sync(0xffffffffu, base, 0);
         if (defer) {
           const int slot = base + __popc(dm & ((1u << lane) - 1u));
-          if (slot < kBuQueue) {
+          if (slot < kBuQueue)
             q_v[slot] = (int)((wb + k) * 32 + lane);
-          } else {
-            long long ex = e[k] + kBuFirst;
-            probe_range<kBuMore, true, ASYNC>(p, fbc, fbn, ex, ee[k], found, found2);
-            defer = false;
-          }
+          else
+            gq[slot - kBuQueue] = (int)((wb + k) * 32 + lane);
         }
       }
       if (ASYNC && act && found < 0 && !defer && found2 < 0) {
@@ -1805,7 +1822,7 @@ __device__ void bottom_up_words(const Params& p, Smem& sm, Acc& acc, int L, cons
     }
   }
   __syncthreads();
-  bu_drain<PAR, ASYNC>(p, sm, acc, L, fbc, fbn, fbn2, kBuFirst);
+  bu_drain<PAR, ASYNC>(p, sm, acc, L, fbc, fbn, fbn2, kBuFirst, gq);
 }
 
 // Word-parallel bottom-up step over head records: the same work split and
@@ -1825,7 +1842,8 @@ __device__ void bottom_up_heads(const Params& p, Smem& sm, Acc& acc, int L, cons
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NWARP = kBlock / 32;
   constexpr long long kStride = (long long)NWARP * kBuWords;
-  int* q_v = &sm.st_id[0][0];  // deferred vertices
+  int* q_v = &sm.st_id[0][0];  // deferred vertices, then (past kBuQueue) the slice's part of p.ulist
+  int* gq = p.ulist + w0 * 32;
   if (threadIdx.x == 0) {
     sm.bu_n = 0;
     sm.bu_next = 0;
@@ -1859,17 +1877,44 @@ __device__ void bottom_up_heads(const Params& p, Smem& sm, Acc& acc, int L, cons
       wc[k][1] = h[k].y >= 0 ? fbc[h[k].y >> 5] : 0u;
       wc[k][2] = h[k].z >= 0 ? fbc[h[k].z >> 5] : 0u;
     }
+    int found[kBuWords], found2[kBuWords];
+    long long d[kBuWords];
+#pragma unroll
+    for (int k = 0; k < kBuWords; ++k) {
+      const bool act = (un[k] >> lane) & 1u;
+      const int u[F] = {h[k].x, h[k].y, h[k].z};
+      found[k] = -1;
+      found2[k] = -1;
+#pragma unroll
+      for (int j = 0; j < F; ++j)
+        if (found[k] < 0 && u[j] >= 0 && ((wc[k][j] >> (u[j] & 31)) & 1u)) found[k] = u[j];
+      d[k] = act ? head_degree(p, h[k], (int)((wb + k) * 32 + lane)) : 0;
+    }
+    if (ASYNC && XBFS_BU_FOUND2) {
+      // a vertex whose whole list is in its head record and has no level-L
+      // parent: a neighbour already in frontier L+1 gives level L+2 (the
+      // words of both vertices read together)
+      uint32_t wn[kBuWords][F];
+#pragma unroll
+      for (int k = 0; k < kBuWords; ++k) {
+        const bool need = ((un[k] >> lane) & 1u) && found[k] < 0 && d[k] <= F;
+        const int u[F] = {h[k].x, h[k].y, h[k].z};
+#pragma unroll
+        for (int j = 0; j < F; ++j) wn[k][j] = (need && u[j] >= 0) ? ld_cg_u32(fbn + (u[j] >> 5)) : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < kBuWords; ++k) {
+        const int u[F] = {h[k].x, h[k].y, h[k].z};
+#pragma unroll
+        for (int j = 0; j < F; ++j)
+          if (found2[k] < 0 && u[j] >= 0 && ((wn[k][j] >> (u[j] & 31)) & 1u)) found2[k] = u[j];
+      }
+    }
 #pragma unroll
     for (int k = 0; k < kBuWords; ++k) {
       const bool act = (un[k] >> lane) & 1u;
       const int v = (int)((wb + k) * 32 + lane);
-      const int u[F] = {h[k].x, h[k].y, h[k].z};
-      int found = -1, found2 = -1;
-#pragma unroll
-      for (int j = 0; j < F; ++j)
-        if (found < 0 && u[j] >= 0 && ((wc[k][j] >> (u[j] & 31)) & 1u)) found = u[j];
-      const long long d = act ? head_degree(p, h[k], v) : 0;
-      bool defer = act && found < 0 && d > F;
+      const bool defer = act && found[k] < 0 && d[k] > F;
       const unsigned dm = __ballot_sync(0xffffffffu, defer);
       if (dm) {
         int base = 0;
@@ -1877,33 +1922,24 @@ __device__ void bottom_up_heads(const Params& p, Smem& sm, Acc& acc, int L, cons
         base = __shfl_sync(0xffffffffu, base, 0);
         if (defer) {
           const int slot = base + __popc(dm & ((1u << lane) - 1u));
-          if (slot < kBuQueue) {
+          if (slot < kBuQueue)
             q_v[slot] = v;
-          } else {
-            const long long e0 = ld_nc_i64(p.beg + v);
-            long long ex = e0 + F;
-            probe_range<kBuMore, true, ASYNC>(p, fbc, fbn, ex, e0 + d, found, found2);
-            defer = false;
-          }
+          else
+            gq[slot - kBuQueue] = v;
         }
       }
-      if (ASYNC && act && found < 0 && !defer && found2 < 0) {
-#pragma unroll
-        for (int j = 0; j < F; ++j)
-          if (found2 < 0 && u[j] >= 0 && ((ld_cg_u32(fbn + (u[j] >> 5)) >> (u[j] & 31)) & 1u)) found2 = u[j];
-      }
-      const bool got1 = act && found >= 0;
-      const bool got2 = ASYNC && act && !got1 && !defer && found2 >= 0;
+      const bool got1 = act && found[k] >= 0;
+      const bool got2 = ASYNC && act && !got1 && !defer && found2[k] >= 0;
       if (got1) {
         p.levels[v] = L + 1;
-        if (PAR) p.parents[v] = found;
+        if (PAR) p.parents[v] = found[k];
         acc.n1 += 1;
-        acc.m1 += d;
+        acc.m1 += d[k];
       } else if (got2) {
         p.levels[v] = L + 2;
-        if (PAR) p.parents[v] = found2;
+        if (PAR) p.parents[v] = found2[k];
         acc.n2 += 1;
-        acc.m2 += d;
+        acc.m2 += d[k];
       }
       const uint32_t m1 = __ballot_sync(0xffffffffu, got1);
       const uint32_t m2 = __ballot_sync(0xffffffffu, got2);
@@ -1916,7 +1952,7 @@ __device__ void bottom_up_heads(const Params& p, Smem& sm, Acc& acc, int L, cons
     }
   }
   __syncthreads();
-  bu_drain<PAR, ASYNC>(p, sm, acc, L, fbc, fbn, fbn2, F);
+  bu_drain<PAR, ASYNC>(p, sm, acc, L, fbc, fbn, fbn2, F, gq);
 }
 
 // Block-reduce the accumulators and publish them to the frontier descriptors.
@@ -2293,7 +2329,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       QOut qo2;
       for (int b2 = 0; b2 < 3; ++b2) qo2.b[b2] = p.q[par][b2];
       qo2.ctr = F2->bin;
-      const bool asyncq = XBFS_ASYNC_QUEUE && p.async_bu && !words && sm.asyncq_ok;
+      const bool asyncq = XBFS_ASYNC_QUEUE && XBFS_BU_ASYNC_LIST && p.async_bu && !words && sm.asyncq_ok;
       if (threadIdx.x == 0 && asyncq) ls.pend_q_for = L + 2;
       if (words && heads) {
         if (p.async_bu)
@@ -2305,7 +2341,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
           bottom_up_words<PAR, true>(p, sm, acc, (int)L, fbc, fbn, fbn2);
         else
           bottom_up_words<PAR, false>(p, sm, acc, (int)L, fbc, fbn, fbn2);
-      } else if (p.async_bu) {
+      } else if (p.async_bu && XBFS_BU_ASYNC_LIST) {
         if (heads)
           bottom_up<PAR, true, true>(p, sm, acc, (int)L, fbc, fbn, fbn2, qo2, asyncq);
         else
