@@ -101,15 +101,22 @@ def collect(graph_specs: list[tuple], sources: int = 4, seed: int = 1, follows=(
     return Dataset(np.concatenate(feats), np.concatenate(labels), np.concatenate(costs))
 
 
-def make_graph(spec: tuple, device: int = 0) -> Graph:
+def make_graph(spec: tuple, device: int = 0, sort: bool = True) -> Graph:
+    """The graph of a spec, neighbours in descending degree order by default
+    (the preparation the bench applies: the per-level costs the switch is
+    trained on should be those of the graphs it runs on)."""
     kind = spec[0]
     if kind == "rmat":
-        return Graph.rmat(spec[1], spec[2], spec[3] if len(spec) > 3 else 1, device=device)
-    if kind == "grid":
-        return Graph.grid(spec[1], spec[2], device=device)
-    if kind == "er":
-        return Graph.er(spec[1], spec[2], spec[3] if len(spec) > 3 else 1, device=device)
-    raise ValueError(spec)
+        g = Graph.rmat(spec[1], spec[2], spec[3] if len(spec) > 3 else 1, device=device)
+    elif kind == "grid":
+        g = Graph.grid(spec[1], spec[2], device=device)
+    elif kind == "er":
+        g = Graph.er(spec[1], spec[2], spec[3] if len(spec) > 3 else 1, device=device)
+    else:
+        raise ValueError(spec)
+    if sort:
+        g.sort_adjacency("degree")
+    return g
 
 
 def init_weights(feats: np.ndarray, seed: int = 0) -> np.ndarray:
