@@ -89,6 +89,11 @@ constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: 
 #ifndef XBFS_MARK_FBN_CHECK
 #define XBFS_MARK_FBN_CHECK 0
 #endif
+// Levels-only two-phase levels mark blindly (no visited test per edge) when
+// frontier L+1 holds no early entries (1), or always test (0).
+#ifndef XBFS_TD_BLIND
+#define XBFS_TD_BLIND 1
+#endif
 // Bins with bitmap output are expanded by gather_bin_warp (1) or in
 // gather_bin's block rounds (0).
 #ifndef XBFS_TD_WARP_GATHER
@@ -615,7 +620,15 @@ __device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int
 // pass the test on several edges before the first reduction lands: its bit
 // is just set more than once.
 template <bool PAR, int N>
-__device__ __forceinline__ void mark_batch(const Params& p, const int (&v)[N], const int (&u)[N], uint32_t* fbn) {
+__device__ __forceinline__ void mark_batch(const Params& p, const int (&v)[N], const int (&u)[N], uint32_t* fbn,
+                                           int mark) {
+  if (!PAR && mark == 2) {
+    // blind marks (see finalize_marks): no test at all
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+      if (v[k] >= 0) red_or_u32(fbn + (v[k] >> 5), 1u << (v[k] & 31));
+    return;
+  }
   uint32_t vw[N], fw[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
@@ -672,7 +685,7 @@ __device__ __forceinline__ int smem_owner(const unsigned* web, int n, unsigned l
 // lanes. The entries are reloaded only when the range passes the 32nd.
 template <bool PAR>
 __device__ void gather_bin_warp(const Params& p, Acc& acc, const QOut& q, const QBin& in, unsigned cnt,
-                                unsigned long long M, int L, uint32_t* fbn, bool qside, bool mark) {
+                                unsigned long long M, int L, uint32_t* fbn, bool qside, int mark) {
   if (cnt == 0 || M == 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NWARP = kBlock / 32;
@@ -707,7 +720,7 @@ __device__ void gather_bin_warp(const Params& p, Acc& acc, const QOut& q, const 
         v[k] = e < rend ? ld_stream_i32(p.csr + bo + (long long)(e - xo)) : -1;
       }
       if (mark)
-        mark_batch<PAR>(p, v, u, fbn);
+        mark_batch<PAR>(p, v, u, fbn, mark);
       else
         claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
     }
@@ -722,7 +735,7 @@ __device__ void gather_bin_warp(const Params& p, Acc& acc, const QOut& q, const 
 // and large bins, and the heavy list of a fused sweep).
 template <bool PAR>
 __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
-                           unsigned long long M, int L, bool enq, uint32_t* fbn, bool qside, bool mark = false) {
+                           unsigned long long M, int L, bool enq, uint32_t* fbn, bool qside, int mark = 0) {
   if (cnt == 0 || M == 0) return;
   if (!enq && (XBFS_TD_WARP_GATHER || mark)) {
     gather_bin_warp<PAR>(p, acc, q, in, cnt, M, L, fbn, qside, mark);
@@ -827,7 +840,7 @@ __device__ void gather_bin(const Params& p, Smem& sm, const QOut& q, Acc& acc, c
 // small_max, so shares of many entries carry similar numbers of edges.
 template <bool PAR>
 __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& acc, const QBin& in, unsigned cnt,
-                               unsigned long long M, int L, bool enq, uint32_t* fbn, bool qside) {
+                               unsigned long long M, int L, bool enq, uint32_t* fbn, bool qside, bool blind = false) {
   if (cnt == 0) return;
   const bool spec = sm.spec != 0;
   const unsigned long long G = gridDim.x, b = blockIdx.x;
@@ -866,7 +879,12 @@ __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& ac
       }
 #pragma unroll
       for (int k = 0; k < kK; ++k)
-        if (v[k] >= 0) claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, enq, fbn, spec, qside);
+        if (v[k] >= 0) {
+          if (blind)
+            red_or_u32(fbn + (v[k] >> 5), 1u << (v[k] & 31));
+          else
+            claim_td<PAR>(p, sm, q, acc, v[k], u[k], L, enq, fbn, spec, qside);
+        }
       __syncthreads();
       if (enq && need_flush(sm)) flush(sm, q);
     }
@@ -883,7 +901,7 @@ __device__ void gather_entries(const Params& p, Smem& sm, const QOut& q, Acc& ac
 template <bool PAR>
 __device__ void gather_entries_warp(const Params& p, const QOut& q, const QBin& in, unsigned cnt,
                                     unsigned long long M, unsigned i0, unsigned i1, int L, bool enq, uint32_t* fbn,
-                                    bool spec, FDesc* f1, bool qside) {
+                                    bool spec, FDesc* f1, bool qside, bool blind = false) {
   const int lane = threadIdx.x & 31;
   const unsigned i = i0 + lane;
   const bool own = i < i1;
@@ -917,6 +935,10 @@ __device__ void gather_entries_warp(const Params& p, const QOut& q, const QBin& 
     const int par_u = __shfl_sync(0xffffffffu, u, lo);
     int v = -1;
     if (e < T) v = ld_stream_i32(p.csr + bg_a + (e - ex_a));
+    if (blind && v >= 0) {  // a blind mark instead of a claim (see finalize_marks)
+      red_or_u32(fbn + (v >> 5), 1u << (v & 31));
+      v = -1;
+    }
     // claim (same rules as claim_td)
     bool win = false;
     long long b0 = 0, b1 = 0;
@@ -1025,7 +1047,7 @@ __device__ __forceinline__ int lane_owner(int ex, int t) {
 constexpr int kWarpSeg = XBFS_TD_WARP_SEG;
 template <bool PAR>
 __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const QOut& q, const uint32_t* fbc, int L,
-                                    uint32_t* fbn, int par, bool qside, bool mark) {
+                                    uint32_t* fbn, int par, bool qside, int mark) {
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
@@ -1070,7 +1092,7 @@ __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const Q
         const int v[3] = {h[j].x, h[j].y, h[j].z};
         const int u[3] = {uu[j], uu[j], uu[j]};
         if (mark)
-          mark_batch<PAR>(p, v, u, fbn);
+          mark_batch<PAR>(p, v, u, fbn, mark);
         else
           claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
       }
@@ -1105,7 +1127,7 @@ __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const Q
           v[k] = e < T ? __ldg(p.csr + wbg[slot] + off) : -1;
         }
         if (mark)
-          mark_batch<PAR>(p, v, u, fbn);
+          mark_batch<PAR>(p, v, u, fbn, mark);
         else
           claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
       }
@@ -1120,7 +1142,7 @@ __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const Q
 // (one per lane), sets their visited bits (one thread per word), and then
 // takes the new vertices 64 at a time, two per lane: level L+1, and the
 // frontier statistics with the degrees from their head records.
-__device__ void finalize_marks(const Params& p, Acc& acc, int L, const uint32_t* fbn) {
+__device__ void finalize_marks(const Params& p, Acc& acc, int L, uint32_t* fbn, bool blind) {
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
   const long long w0 = nw * b / G, w1 = nw * (b + 1) / G;
@@ -1134,6 +1156,7 @@ __device__ void finalize_marks(const Params& p, Acc& acc, int L, const uint32_t*
         const uint32_t vv = ld_cg_u32(p.vis + c + lane);
         nb = f & ~vv;
         if (nb) p.vis[c + lane] = vv | nb;
+        if (blind && nb != f) fbn[c + lane] = nb;  // blind marks of visited targets
       }
     }
     const int pc = __popc(nb);
@@ -2255,7 +2278,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       // and the heavy list; the small bin still claims), then, after a
       // barrier, finalize_marks: levels, visited bits and statistics of the
       // marked vertices that no claim took
-      const bool mark = XBFS_TD_MARK && !enq && p.head && sm.mark_ok && !qside;
+      // Without parents and with no early (asynchronous) entries in frontier
+      // L+1's bitmap, the marks are blind: every edge sets its target's bit
+      // with no read of the visited bitmap (on these levels nearly every
+      // target is unvisited), and finalize_marks also clears the bits of
+      // visited targets; claims then make way for marks in every expansion
+      // path of the level, so no visited bit is set before the finalize.
+      const int mark = !(XBFS_TD_MARK && !enq && p.head && sm.mark_ok && !qside)
+                           ? 0
+                           : ((!PAR && XBFS_TD_BLIND && sm.pend_next == 0) ? 2 : 1);
       QOut qo;
       for (int b2 = 0; b2 < 3; ++b2) qo.b[b2] = p.q[par ^ 1][b2];
       qo.ctr = F1->bin;
@@ -2269,7 +2300,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       if (tiny) {
         if (threadIdx.x < 32 && i1 > i0)
           gather_entries_warp<PAR>(p, qo, p.q[par][0], cnt0, pk0 >> 31, i0, i1, (int)L, enq, fbn, sm.spec != 0, F1,
-                                   qside);
+                                   qside, mark == 2);
       } else {
         if (q_valid) {
           for (int bin = 2; bin >= 1; --bin) {
@@ -2277,7 +2308,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
             gather_bin<PAR>(p, sm, qo, acc, p.q[par][bin], (unsigned)(pk & kCountMask), pk >> 31, (int)L, enq, fbn,
                             qside, mark);
           }
-          gather_entries<PAR>(p, sm, qo, acc, p.q[par][0], cnt0, pk0 >> 31, (int)L, enq, fbn, qside);
+          gather_entries<PAR>(p, sm, qo, acc, p.q[par][0], cnt0, pk0 >> 31, (int)L, enq, fbn, qside, mark == 2);
         } else if ((XBFS_TD_HEADS || mark) && !enq && p.head) {
           expand_bitmap_heads<PAR>(p, sm, acc, qo, fbc, (int)L, fbn, par, qside, mark);
         } else {
@@ -2300,7 +2331,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         }
       }
       if (mark) {
-        finalize_marks(p, acc, (int)L, fbn);
+        finalize_marks(p, acc, (int)L, fbn, mark == 2);
         publish_acc(sm, acc, F1, nullptr);
         if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       }
