@@ -94,6 +94,12 @@ constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: 
 #ifndef XBFS_TD_BLIND
 #define XBFS_TD_BLIND 1
 #endif
+// Two-phase levels need at least V / XBFS_MARK_NU_DIV unvisited vertices
+// (and V/2 frontier edges); marking the large levels with few unvisited
+// vertices too (a divisor of 2^20) measured slower on R-MAT scale 23.
+#ifndef XBFS_MARK_NU_DIV
+#define XBFS_MARK_NU_DIV 16
+#endif
 // Bins with bitmap output are expanded by gather_bin_warp (1) or in
 // gather_bin's block rounds (0).
 #ifndef XBFS_TD_WARP_GATHER
@@ -446,6 +452,34 @@ __device__ __forceinline__ void direct_enqueue(const QBin& q, unsigned long long
   q.ids[slot] = v;
   q.eb[slot] = (unsigned)(old >> 31);
   q.bg[slot] = bg;
+}
+
+// Vertices of the lanes with `have` (degree d > 0, CSR offset b0) into a
+// binned queue: per bin one packed atomic for the warp (edges << 31 |
+// count), entries at consecutive slots. Called by a full warp.
+__device__ __forceinline__ void enqueue_warp(const Params& p, const QOut& q2, bool have, int v, long long d,
+                                             long long b0) {
+  const int lane = threadIdx.x & 31;
+  have = have && d > 0;
+  if (!__ballot_sync(0xffffffffu, have)) return;
+  const int bin = have ? bin_of(d, p.small_max, p.medium_max) : -1;
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    const bool mine = bin == b;
+    const unsigned mask = __ballot_sync(0xffffffffu, mine);
+    if (!mask) continue;
+    const long long dd = mine ? d : 0;
+    const long long inc = warp_inclusive_scan(dd);
+    unsigned long long old = 0;
+    if (lane == 31) old = atomicAdd(&q2.ctr[b], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
+    old = __shfl_sync(0xffffffffu, old, 31);
+    if (mine) {
+      const unsigned long long slot = (old & kCountMask) + __popc(mask & ((1u << lane) - 1));
+      q2.b[b].ids[slot] = v;
+      q2.b[b].eb[slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - dd));
+      q2.b[b].bg[slot] = b0;
+    }
+  }
 }
 
 __device__ __forceinline__ void stage(Smem& sm, const QOut& q, int bin, int v, long long d, long long bg) {
@@ -1387,34 +1421,6 @@ __device__ __forceinline__ void probe_pair(const Params& p, const uint32_t* fbc,
   }
 }
 
-// Level-(L+2) winners of the asynchronous bottom-up rule (lanes with `have`)
-// into frontier L+2's binned queue: per bin one packed atomic for the warp
-// (edges << 31 | count), entries at consecutive slots. Called by a full warp.
-__device__ __forceinline__ void queue_early_warp(const Params& p, const QOut& q2, bool have, int v, long long d,
-                                                 long long b0) {
-  const int lane = threadIdx.x & 31;
-  have = have && d > 0;
-  if (!__ballot_sync(0xffffffffu, have)) return;
-  const int bin = have ? bin_of(d, p.small_max, p.medium_max) : -1;
-#pragma unroll
-  for (int b = 0; b < 3; ++b) {
-    const bool mine = bin == b;
-    const unsigned mask = __ballot_sync(0xffffffffu, mine);
-    if (!mask) continue;
-    const long long dd = mine ? d : 0;
-    const long long inc = warp_inclusive_scan(dd);
-    unsigned long long old = 0;
-    if (lane == 31) old = atomicAdd(&q2.ctr[b], ((unsigned long long)inc << 31) | (unsigned long long)__popc(mask));
-    old = __shfl_sync(0xffffffffu, old, 31);
-    if (mine) {
-      const unsigned long long slot = (old & kCountMask) + __popc(mask & ((1u << lane) - 1));
-      q2.b[b].ids[slot] = v;
-      q2.b[b].eb[slot] = (unsigned)((old >> 31) + (unsigned long long)(inc - dd));
-      q2.b[b].bg[slot] = b0;
-    }
-  }
-}
-
 // Publishes a warp's bottom-up results for 32 consecutive entries of a sorted
 // list: vertices sharing a bitmap word sit in adjacent lanes, so their bits
 // are ORed along each run of equal words and the run's first lane issues one
@@ -1545,7 +1551,7 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
             acc.m2 += ee[j] - eb[j];
           }
         }
-        if (ASYNC && asyncq) queue_early_warp(p, q2, m2 != 0, v[j], ee[j] - eb[j], eb[j]);
+        if (ASYNC && asyncq) enqueue_warp(p, q2, m2 != 0, v[j], ee[j] - eb[j], eb[j]);
         bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, m2, v[j] >= 0);
       }
     }
@@ -1626,7 +1632,7 @@ __device__ void bottom_up(const Params& p, Smem& sm, Acc& acc, int L, const uint
         acc.m2 += e1 - e0;
       }
     }
-    if (ASYNC && asyncq) queue_early_warp(p, q2, m2 != 0, v, e1 - e0, e0);
+    if (ASYNC && asyncq) enqueue_warp(p, q2, m2 != 0, v, e1 - e0, e0);
     // The warp's 32 vertices are consecutive entries of a sorted list, so
     // vertices sharing a bitmap word sit in adjacent lanes: OR their bits
     // along each run of equal words and let the run's first lane publish
@@ -2185,7 +2191,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         if (m_u < 0) m_u = 0;
         sm.bu_dense = (n_u * 4 >= p.V) ? 1 : 0;
         sm.asyncq_ok = (n_u * 4 < p.V) ? 1 : 0;
-        sm.mark_ok = (n_u * 16 >= p.V && m_f * 2 >= p.V) ? 1 : 0;
+        sm.mark_ok = (n_u * XBFS_MARK_NU_DIV >= p.V && m_f * 2 >= p.V) ? 1 : 0;
         sm.qside_ok = (n_u * 64 <= p.V && (pn == 0 || ls.pend_q_for == L + 1)) ? 1 : 0;
         switch (p.policy) {
           case XBFS_POLICY_FORCED: {
