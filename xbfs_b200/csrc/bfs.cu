@@ -94,6 +94,17 @@ constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: 
 #ifndef XBFS_TD_BLIND
 #define XBFS_TD_BLIND 1
 #endif
+// The head neighbours of a frontier sweep are claimed through
+// claim_filtered, six visited words read together (1), or as two batches of
+// three through claim_batch (0).
+#ifndef XBFS_TD_HEAD_FILTER
+#define XBFS_TD_HEAD_FILTER 1
+#endif
+// The rest of the sweep's segments is claimed through claim_filtered (1) or
+// claim_batch (0).
+#ifndef XBFS_TD_REM_FILTER
+#define XBFS_TD_REM_FILTER 0
+#endif
 // Two-phase levels need at least V / XBFS_MARK_NU_DIV unvisited vertices
 // (and V/2 frontier edges); marking the large levels with few unvisited
 // vertices too (a divisor of 2^20) measured slower on R-MAT scale 23.
@@ -642,6 +653,36 @@ __device__ __forceinline__ void claim_batch(const Params& p, Acc& acc, const int
     }
 }
 
+// Top-down claims of N targets where few are expected to be unvisited (the
+// head neighbours of a frontier sweep late in the traversal): the visited
+// words of all N are read together, and the targets that look unvisited are
+// then claimed one after another (the atomic, the winner's writes and CSR
+// offsets), which keeps fewer registers live than claim_batch.
+template <bool PAR, int N>
+__device__ __forceinline__ void claim_filtered(const Params& p, Acc& acc, const int (&v)[N], const int (&u)[N], int L,
+                                               uint32_t* fbn, const QOut& q, bool qside) {
+  uint32_t vw[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) vw[k] = (v[k] >= 0) ? ld_cg_u32(p.vis + (v[k] >> 5)) : ~0u;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    if (v[k] < 0 || ((vw[k] >> (v[k] & 31)) & 1u)) continue;
+    const uint32_t bit = 1u << (v[k] & 31);
+    if (atomicOr(p.vis + (v[k] >> 5), bit) & bit) continue;
+    p.levels[v[k]] = L + 1;
+    if (PAR) p.parents[v[k]] = u[k];
+    red_or_u32(fbn + (v[k] >> 5), bit);
+    const long long b0 = ld_nc_i64(p.beg + v[k]);
+    const long long d = ld_nc_i64(p.beg + v[k] + 1) - b0;
+    acc.n1 += 1;
+    acc.m1 += d;
+    if (qside && d > 0) {
+      const int bin = bin_of(d, p.small_max, p.medium_max);
+      direct_enqueue(q.b[bin], &q.ctr[bin], v[k], d, b0);
+    }
+  }
+}
+
 // Marking form of claim_batch for a top-down level with many fresh targets
 // (two-phase level): a target that is not visited (and, with
 // XBFS_MARK_FBN_CHECK, not yet in frontier L+1's bitmap) gets its bit there
@@ -1121,14 +1162,24 @@ __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const Q
         bg[j] = rem > 0 ? ld_nc_i64(p.beg + uu[j]) + 3 : 0;
         r[j] = rem > kWarpSeg ? -1 : (rem > 0 ? (int)rem : 0);
       }
+      if (mark) {
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int v[3] = {h[j].x, h[j].y, h[j].z};
-        const int u[3] = {uu[j], uu[j], uu[j]};
-        if (mark)
+        for (int j = 0; j < 2; ++j) {
+          const int v[3] = {h[j].x, h[j].y, h[j].z};
+          const int u[3] = {uu[j], uu[j], uu[j]};
           mark_batch<PAR>(p, v, u, fbn, mark);
-        else
+        }
+      } else if (XBFS_TD_HEAD_FILTER) {
+        const int v[6] = {h[0].x, h[0].y, h[0].z, h[1].x, h[1].y, h[1].z};
+        const int u[6] = {uu[0], uu[0], uu[0], uu[1], uu[1], uu[1]};
+        claim_filtered<PAR>(p, acc, v, u, L, fbn, q, qside);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int v[3] = {h[j].x, h[j].y, h[j].z};
+          const int u[3] = {uu[j], uu[j], uu[j]};
           claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
+        }
       }
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
@@ -1162,6 +1213,8 @@ __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const Q
         }
         if (mark)
           mark_batch<PAR>(p, v, u, fbn, mark);
+        else if (XBFS_TD_REM_FILTER)
+          claim_filtered<PAR>(p, acc, v, u, L, fbn, q, qside);
         else
           claim_batch<PAR>(p, acc, v, u, L, fbn, q, qside);
       }
