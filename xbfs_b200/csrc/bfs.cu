@@ -111,6 +111,14 @@ constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: 
 #ifndef XBFS_MARK_NU_DIV
 #define XBFS_MARK_NU_DIV 16
 #endif
+// gather_bin_warp reads a chunk of edges that lies in one segment with
+// 16-byte CSR loads (1) or one 4-byte load per edge (0). Measured equal on
+// the hub levels of R-MAT scale 23 (188-192 us either way): a warp's CSR
+// reads are one coalesced request per 32 edges against 32 random visited-
+// word reads or reductions, so the CSR is not what bounds these levels.
+#ifndef XBFS_TD_VEC
+#define XBFS_TD_VEC 0
+#endif
 // Bins with bitmap output are expanded by gather_bin_warp (1) or in
 // gather_bin's block rounds (0).
 #ifndef XBFS_TD_WARP_GATHER
@@ -778,21 +786,54 @@ __device__ void gather_bin_warp(const Params& p, Acc& acc, const QOut& q, const 
     if (lane == 31 && slot + 1 < cnt) wend = in.eb[slot + 1];
     wend = __shfl_sync(0xffffffffu, wend, 31);
     const unsigned long long rend = wend < hi ? wend : hi;
-    for (; r < rend; r += 32 * kTdIlp) {
+    for (; r < rend;) {
       int v[kTdIlp], u[kTdIlp];
-#pragma unroll
-      for (int k = 0; k < kTdIlp; ++k) {
-        const unsigned long long e = r + 32 * k + lane;
-        int o = 0;  // last lane whose entry starts at or before e
+      const unsigned long long cend = r + 32 * kTdIlp < rend ? r + 32 * kTdIlp : rend;
+      int o0 = 0, o1 = 0;  // owners of the chunk's first and last edges
+      if (XBFS_TD_VEC) {
 #pragma unroll
         for (int st = 16; st > 0; st >>= 1) {
-          const unsigned x = __shfl_sync(0xffffffffu, eb, o + st);
-          if ((unsigned long long)x <= e) o += st;
+          const unsigned x0 = __shfl_sync(0xffffffffu, eb, o0 + st);
+          const unsigned x1 = __shfl_sync(0xffffffffu, eb, o1 + st);
+          if ((unsigned long long)x0 <= r) o0 += st;
+          if ((unsigned long long)x1 <= cend - 1) o1 += st;
         }
-        const unsigned xo = __shfl_sync(0xffffffffu, eb, o);
-        const long long bo = __shfl_sync(0xffffffffu, bg, o);
-        u[k] = __shfl_sync(0xffffffffu, id, o);
-        v[k] = e < rend ? ld_stream_i32(p.csr + bo + (long long)(e - xo)) : -1;
+      }
+      if (XBFS_TD_VEC && kTdIlp == 4 && o0 == o1) {
+        // one segment: 16-byte loads from the aligned CSR index at or below
+        // the chunk's first edge, lane l the four entries from 4l; the
+        // chunk ends where the 32 vectors end
+        const unsigned xo = __shfl_sync(0xffffffffu, eb, o0);
+        const long long bo = __shfl_sync(0xffffffffu, bg, o0);
+        const int uo = __shfl_sync(0xffffffffu, id, o0);
+        const long long a0 = bo + (long long)(r - xo), aend = a0 + (long long)(cend - r);
+        const long long al = a0 & ~3ll, my = al + 4 * lane;
+        int4 x = make_int4(-1, -1, -1, -1);
+        if (my < aend) x = ld_stream_v4(p.csr + my);
+        const int xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int k = 0; k < kTdIlp; ++k) {
+          v[k] = (my + k >= a0 && my + k < aend) ? xs[k] : -1;
+          u[k] = uo;
+        }
+        const long long cov = (al + 32 * kTdIlp < aend ? al + 32 * kTdIlp : aend) - a0;
+        r += (unsigned long long)cov;
+      } else {
+#pragma unroll
+        for (int k = 0; k < kTdIlp; ++k) {
+          const unsigned long long e = r + 32 * k + lane;
+          int o = 0;  // last lane whose entry starts at or before e
+#pragma unroll
+          for (int st = 16; st > 0; st >>= 1) {
+            const unsigned x = __shfl_sync(0xffffffffu, eb, o + st);
+            if ((unsigned long long)x <= e) o += st;
+          }
+          const unsigned xo = __shfl_sync(0xffffffffu, eb, o);
+          const long long bo = __shfl_sync(0xffffffffu, bg, o);
+          u[k] = __shfl_sync(0xffffffffu, id, o);
+          v[k] = e < rend ? ld_stream_i32(p.csr + bo + (long long)(e - xo)) : -1;
+        }
+        r = cend;
       }
       if (mark)
         mark_batch<PAR>(p, v, u, fbn, mark);

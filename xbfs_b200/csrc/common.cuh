@@ -82,6 +82,14 @@ __device__ __forceinline__ int4 ld_nc_na_v4(const int4* p) {
       : "l"(p));
   return v;
 }
+// 16-byte form of ld_stream_i32 (p 16-byte aligned).
+__device__ __forceinline__ int4 ld_stream_v4(const int* p) {
+  int4 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(p), "l"(l2_policy_evict_first()));
+  return v;
+}
 __device__ __forceinline__ long long ld_nc_i64(const long long* p) {
   long long v;
   asm volatile("ld.global.nc.b64 %0, [%1];" : "=l"(v) : "l"(p));
