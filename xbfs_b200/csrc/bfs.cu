@@ -105,6 +105,11 @@ constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: 
 #ifndef XBFS_TD_REM_FILTER
 #define XBFS_TD_REM_FILTER 0
 #endif
+// Bottom-up levels with at least V / XBFS_BU_DENSE_DIV unvisited vertices
+// are word-parallel, sparser ones probe a compacted list.
+#ifndef XBFS_BU_DENSE_DIV
+#define XBFS_BU_DENSE_DIV 4
+#endif
 // Two-phase levels need at least V / XBFS_MARK_NU_DIV unvisited vertices
 // (and V/2 frontier edges); marking the large levels with few unvisited
 // vertices too (a divisor of 2^20) measured slower on R-MAT scale 23.
@@ -2283,7 +2288,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
         long long m_u = p.E - ls.vis_m - pm;
         if (n_u < 0) n_u = 0;
         if (m_u < 0) m_u = 0;
-        sm.bu_dense = (n_u * 4 >= p.V) ? 1 : 0;
+        sm.bu_dense = (n_u * XBFS_BU_DENSE_DIV >= p.V) ? 1 : 0;
         sm.asyncq_ok = (n_u * 4 < p.V) ? 1 : 0;
         sm.mark_ok = (n_u * XBFS_MARK_NU_DIV >= p.V && m_f * 2 >= p.V) ? 1 : 0;
         sm.qside_ok = (n_u * 64 <= p.V && (pn == 0 || ls.pend_q_for == L + 1)) ? 1 : 0;
