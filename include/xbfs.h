@@ -155,7 +155,12 @@ void xbfs_opts_init(xbfs_opts* o);
 xbfs_status xbfs_graph_load(const char* beg_path, const char* csr_path, int32_t device,
                             xbfs_graph** out);
 /* Upload a host CSR (same layout). Replaces the cudaMalloc/cudaMemcpy of
- * beg_cu/csr_cu in main (bfs_gpu_update.cu:175-180). */
+ * beg_cu/csr_cu in main (bfs_gpu_update.cu:175-180). Every graph handle
+ * (loaded, uploaded or generated) also keeps one 16-byte head record per
+ * vertex on the device (its first three neighbours in CSR order and its
+ * degree), which the traversal's bottom-up probes and bitmap sweeps read
+ * instead of the CSR offsets and the segment's first sector: device memory
+ * is 8(V+1) + 4E + 16V bytes plus the traversal workspace. */
 xbfs_status xbfs_graph_upload(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E,
                               int32_t device, xbfs_graph** out);
 xbfs_status xbfs_graph_info(const xbfs_graph* g, int64_t* V, int64_t* E, int64_t* max_degree,
@@ -169,7 +174,8 @@ xbfs_status xbfs_graph_download(const xbfs_graph* g, int64_t* beg, int32_t* csr)
  * parent in fewer probes; XBFS_ADJ_ID_ASC restores ascending ids. Levels
  * never depend on the order (parents may). No reference counterpart: the
  * reference traverses the file order. Needs about 20 bytes per edge of
- * temporary device memory; xbfs_graph_download returns the new order. */
+ * temporary device memory; xbfs_graph_download returns the new order, and
+ * the head records are rewritten to match it. */
 enum { XBFS_ADJ_ID_ASC = 0, XBFS_ADJ_DEGREE_DESC = 1 };
 xbfs_status xbfs_graph_sort_adjacency(xbfs_graph* g, int32_t order);
 /* Write the handle's CSR in the reference's file format. */
