@@ -264,6 +264,30 @@ def test_top_down_levels_with_many_fresh_targets(schedule):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("grid_dim", [1, 2, 7])
+def test_few_ctas_large_shares(grid_dim):
+    """With the grid capped to a few CTAs every CTA owns tens of thousands of
+    vertices: bottom-up steps defer more vertices than the shared-memory queue
+    holds (the rest go to the CTA's part of the list area), the warp-level
+    top-down loops and the two-phase levels walk long shares; levels equal the
+    oracle's and parents form a valid tree in every schedule."""
+    beg, csr = gen_rmat_host(16, 16, 31)
+    g = Graph.from_csr(beg, csr)
+    g.sort_adjacency("degree")
+    b2, c2 = g.download()
+    for s in pick_sources(b2, 3, 12):
+        ref = oracle.bfs_queue(b2, c2, int(s))
+        for kw in ({}, {"policy": "forced", "forced": ["td_queue", "bu"]},
+                   {"policy": "forced", "forced": ["td_queue", "td_queue", "td_scan", "bu", "td_scan"]}):
+            for par in (True, False):
+                r = g.bfs(int(s), want_parents=par, grid_dim=grid_dim, **kw)
+                assert np.array_equal(r.levels, ref), (grid_dim, kw, par)
+                if par:
+                    assert oracle.check_tree(b2, c2, int(s), r.levels, r.parents) == 0
+    g.free()
+
+
+@pytest.mark.gpu
 def test_bottom_up_probe_mode_out_of_range_is_refused():
     beg, csr = gen_rmat_host(10, 8, 2)
     g = Graph.from_csr(beg, csr)

@@ -124,6 +124,11 @@ constexpr int kRoundsNoStage = 4;   // edge-balanced rounds with bitmap output: 
 #ifndef XBFS_TD_VEC
 #define XBFS_TD_VEC 0
 #endif
+// Queue-output levels of symmetric graphs take the next frontier's counts
+// from its bins (1) or publish them with atomics (0).
+#ifndef XBFS_NM_FROM_BINS
+#define XBFS_NM_FROM_BINS 1
+#endif
 // Bins with bitmap output are expanded by gather_bin_warp (1) or in
 // gather_bin's block rounds (0).
 #ifndef XBFS_TD_WARP_GATHER
@@ -154,7 +159,7 @@ struct FDesc {
   unsigned long long m;       // sum of their degrees
   unsigned long long pend_n;  // part found early by asynchronous bottom-up
   unsigned long long pend_m;
-  unsigned long long pad;
+  unsigned long long pad;     // 1: n and m are not published, the bins hold the frontier
 };
 
 struct LevelRecDev {
@@ -1115,6 +1120,7 @@ __device__ void gather_entries_warp(const Params& p, const QOut& q, const QBin& 
       }
     }
   }
+  if (!f1) return;  // the next frontier's counts come from its bins
   n1 = warp_sum(n1);
   m1 = warp_sum(m1);
   if (lane == 0) {
@@ -2083,14 +2089,19 @@ __device__ void bottom_up_heads(const Params& p, Smem& sm, Acc& acc, int L, cons
   bu_drain<PAR, ASYNC>(p, sm, acc, L, fbc, fbn, fbn2, F, gq);
 }
 
-// Block-reduce the accumulators and publish them to the frontier descriptors.
+// Block-reduce the accumulators and publish them to the frontier descriptors
+// (f1 and f2 null: nothing to publish, the accumulators are reset).
 __device__ void publish_acc(Smem& sm, Acc& acc, FDesc* f1, FDesc* f2) {
+  if (!f1 && !f2) {
+    acc = Acc{0, 0, 0, 0};
+    return;
+  }
   long long v[4] = {acc.n1, acc.m1, acc.n2, acc.m2};
   block_sum_n<kBlock, 4, long long>(v, sm.red4);
   const long long n1 = v[0], m1 = v[1], n2 = v[2], m2 = v[3];
   if (threadIdx.x == 0) {
-    if (n1) atomicAdd(&f1->n, (unsigned long long)n1);
-    if (m1) atomicAdd(&f1->m, (unsigned long long)m1);
+    if (f1 && n1) atomicAdd(&f1->n, (unsigned long long)n1);
+    if (f1 && m1) atomicAdd(&f1->m, (unsigned long long)m1);
     if (f2 && n2) {
       atomicAdd(&f2->n, (unsigned long long)n2);
       atomicAdd(&f2->m, (unsigned long long)m2);
@@ -2266,13 +2277,25 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
     FDesc* F3 = &ctl->fd[(L + 3) & 3];
     if (threadIdx.x == 0) {
       // every descriptor word this level needs, loaded together
-      const long long n_f = (long long)ld_cg_u64(&F0->n);
-      const long long m_f = (long long)ld_cg_u64(&F0->m);
+      long long n_f = (long long)ld_cg_u64(&F0->n);
+      long long m_f = (long long)ld_cg_u64(&F0->m);
       const long long pn = (long long)ld_cg_u64(&F1->pend_n);
       const long long pm = (long long)ld_cg_u64(&F1->pend_m);
       const long long own_pend = (long long)ld_cg_u64(&F0->pend_n);
+      const bool from_bins = ld_cg_u64(&F0->pad) != 0;
 #pragma unroll
       for (int b2 = 0; b2 < 3; ++b2) sm.bins[b2] = ld_cg_u64(&F0->bin[b2]);
+      if (from_bins) {
+        // a queue-output level of a symmetric graph: every vertex it found
+        // has a neighbour, so its bins hold the whole frontier
+        n_f = 0;
+        m_f = 0;
+#pragma unroll
+        for (int b2 = 0; b2 < 3; ++b2) {
+          n_f += (long long)(sm.bins[b2] & kCountMask);
+          m_f += (long long)(sm.bins[b2] >> 31);
+        }
+      }
       sm.pend_next = pn;
       sm.spec = m_f <= kSpecEdges ? 1 : 0;
       int s = -1;
@@ -2377,6 +2400,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       // so a small next level expands the queue instead of sweeping the
       // bitmap (the bitmap stays valid too)
       const bool qside = !enq && sm.qside_ok;
+      // A queue-output level of a symmetric graph publishes no frontier
+      // counts: every vertex it finds has degree > 0 and lands in a bin, so
+      // the next decision sums the bins (flagged in the descriptor's last
+      // word) and the level saves the count atomics before its barrier.
+      // Stepped launches keep the counts (the host reads them).
+      const bool nm_bins = XBFS_NM_FROM_BINS && enq && p.allow_bu && p.fresh;
+      FDesc* P1 = nm_bins ? nullptr : F1;
+      if (nm_bins && blockIdx.x == 0 && threadIdx.x == 0) F1->pad = 1ull;
       // A level with bitmap output and many unvisited vertices runs in two
       // phases: marks of fresh targets into frontier L+1's bitmap without
       // atomics that return (the bitmap sweep, the medium and large bins
@@ -2404,7 +2435,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
       const bool tiny = q_valid && (sm.bins[1] & kCountMask) == 0 && (sm.bins[2] & kCountMask) == 0 && i1 - i0 <= 32;
       if (tiny) {
         if (threadIdx.x < 32 && i1 > i0)
-          gather_entries_warp<PAR>(p, qo, p.q[par][0], cnt0, pk0 >> 31, i0, i1, (int)L, enq, fbn, sm.spec != 0, F1,
+          gather_entries_warp<PAR>(p, qo, p.q[par][0], cnt0, pk0 >> 31, i0, i1, (int)L, enq, fbn, sm.spec != 0, P1,
                                    qside, mark == 2);
       } else {
         if (q_valid) {
@@ -2420,7 +2451,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
           expand_bitmap<PAR>(p, sm, qo, acc, fbc, (int)L, enq, fbn, par, qside);
         }
         if (enq) flush(sm, qo);
-        publish_acc(sm, acc, F1, nullptr);
+        publish_acc(sm, acc, P1, nullptr);
       }
       if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
       if (!q_valid) {
@@ -2431,7 +2462,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_bfs(Params p) {
           gather_bin<PAR>(p, sm, qo, acc, p.heavy, (unsigned)(hk & kCountMask), hk >> 31, (int)L, enq, fbn, qside,
                           mark);
           if (enq) flush(sm, qo);
-          publish_acc(sm, acc, F1, nullptr);
+          publish_acc(sm, acc, P1, nullptr);
           if (!grid_sync(&ctl->bar, nb, epoch, p.timeout_ns)) break;
         }
       }
