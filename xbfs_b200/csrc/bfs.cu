@@ -1800,13 +1800,6 @@ constexpr bool kBuPrefetch = XBFS_BU_PREFETCH;
 #ifndef XBFS_BU_ASYNC_DRAIN
 #define XBFS_BU_ASYNC_DRAIN 0
 #endif
-// Without the level-(L+2) rule the drain of deferred vertices is
-// edge-balanced over each warp (1) or one vertex per lane (0). Measured equal
-// on R-MAT scale 23 (whose deferred lists are short); the balanced form keeps
-// a long list from holding its warp on graphs where they are not.
-#ifndef XBFS_BU_DRAIN_BALANCED
-#define XBFS_BU_DRAIN_BALANCED 1
-#endif
 
 // Second phase of the word-parallel bottom-up step: the vertices deferred to
 // the CTA's shared-memory queue (their first `first` neighbours probed
@@ -1817,76 +1810,6 @@ __device__ void bu_drain(const Params& p, Smem& sm, Acc& acc, int L, const uint3
   const int lane = threadIdx.x & 31;
   const int* q_v = &sm.st_id[0][0];
   const int nq = sm.bu_n;
-  if (!(ASYNC && XBFS_BU_ASYNC_DRAIN) && XBFS_BU_DRAIN_BALANCED) {
-    // Edge-balanced: a warp takes 32 deferred vertices and probes the rest
-    // of their 32 lists together, 32 x kTdIlp neighbours per step spread
-    // evenly over the lanes (owner search over the lanes), so a long list
-    // no longer holds its warp; a hit records its vertex's parent in the
-    // warp's shared slots (any hit is a valid parent). The warp stops when
-    // every vertex of the batch has one.
-    int* par_s = sm.wu + (threadIdx.x >> 5) * 32;
-    for (;;) {
-      int base = 0;
-      if (lane == 0) base = atomicAdd(&sm.bu_next, 32);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if (base >= nq) break;
-      const int i = base + lane;
-      int v = -1;
-      long long e0 = 0, e1 = 0;
-      if (i < nq) {
-        v = i < kBuQueue ? q_v[i] : gq[i - kBuQueue];
-        e0 = ld_nc_i64(p.beg + v);
-        e1 = ld_nc_i64(p.beg + v + 1);
-      }
-      const long long rem = v >= 0 ? e1 - e0 - first : 0;
-      par_s[lane] = -1;
-      __syncwarp();
-      const long long incl = warp_inclusive_scan(rem);
-      const long long ex = incl - rem;
-      const long long T = __shfl_sync(0xffffffffu, incl, 31);
-      for (long long eb = 0; eb < T; eb += 32 * kTdIlp) {
-        int u[kTdIlp], o[kTdIlp];
-#pragma unroll
-        for (int k = 0; k < kTdIlp; ++k) {
-          const long long e = eb + 32 * k + lane;
-          int lo = 0;  // last lane whose list starts at or before e
-#pragma unroll
-          for (int st = 16; st > 0; st >>= 1) {
-            const long long x = __shfl_sync(0xffffffffu, ex, lo + st);
-            if (x <= e) lo += st;
-          }
-          const long long xo = __shfl_sync(0xffffffffu, ex, lo);
-          const long long bo = __shfl_sync(0xffffffffu, e0, lo);
-          o[k] = lo;
-          u[k] = e < T ? __ldg(p.csr + bo + first + (e - xo)) : -1;
-        }
-        uint32_t wc[kTdIlp];
-#pragma unroll
-        for (int k = 0; k < kTdIlp; ++k) wc[k] = u[k] >= 0 ? fbc[u[k] >> 5] : 0u;
-#pragma unroll
-        for (int k = 0; k < kTdIlp; ++k)
-          if (u[k] >= 0 && ((wc[k] >> (u[k] & 31)) & 1u)) par_s[o[k]] = u[k];
-        __syncwarp();
-        if (__all_sync(0xffffffffu, v < 0 || par_s[lane] >= 0)) break;
-      }
-      __syncwarp();
-      const int found = v >= 0 ? par_s[lane] : -1;
-      uint32_t word = 0xffffffffu, m1 = 0;
-      if (v >= 0) {
-        word = (uint32_t)v >> 5;
-        if (found >= 0) {
-          p.levels[v] = L + 1;
-          if (PAR) p.parents[v] = found;
-          m1 = 1u << (v & 31);
-          acc.n1 += 1;
-          acc.m1 += e1 - e0;
-        }
-      }
-      bu_publish_words<ASYNC>(p, fbn, fbn2, word, m1, 0u, v >= 0);
-      __syncwarp();  // the next batch rewrites the warp's slots
-    }
-    return;
-  }
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&sm.bu_next, 32);
