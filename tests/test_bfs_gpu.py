@@ -287,6 +287,42 @@ def test_few_ctas_large_shares(grid_dim):
     g.free()
 
 
+def _directed_rmat(scale, ef, seed):
+    """An asymmetric CSR from an R-MAT graph: edge u->v kept when u < v or
+    u + v is even (so many edges exist one way only)."""
+    beg, csr = gen_rmat_host(scale, ef, seed)
+    src = np.repeat(np.arange(len(beg) - 1, dtype=np.int64), np.diff(beg))
+    keep = (src < csr) | (((src + csr) & 1) == 0)
+    src, dst = src[keep], csr[keep]
+    nb = np.zeros(len(beg), dtype=np.int64)
+    np.add.at(nb, src + 1, 1)
+    return np.cumsum(nb), dst.astype(np.int32)
+
+
+@pytest.mark.gpu
+def test_directed_power_law_top_down_paths():
+    """A directed power-law CSR (bottom-up never allowed): the warp-level
+    sweeps over head records, the two-phase levels (their degree counts come
+    from head records, claims stay) and the queue levels (counts published,
+    not taken from the bins, since a reached vertex may have no out-edge)
+    give the oracle's levels and a valid tree."""
+    beg, csr = _directed_rmat(15, 16, 8)
+    g = Graph.from_csr(beg, csr)
+    g.sort_adjacency("degree")
+    b2, c2 = g.download()
+    for s in pick_sources(b2, 3, 2):
+        ref = oracle.bfs_queue(b2, c2, int(s))
+        for kw in ({}, {"policy": "forced", "forced": ["td_queue", "td_scan"]},
+                   {"policy": "forced", "forced": ["td_scan"]}):
+            r = g.bfs(int(s), want_parents=True, **kw)
+            assert np.array_equal(r.levels, ref), kw
+            assert oracle.check_tree(b2, c2, int(s), r.levels, r.parents) == 0
+            assert r.strategies["bu"] == 0
+            r2 = g.bfs(int(s), **kw)
+            assert np.array_equal(r2.levels, ref), kw
+    g.free()
+
+
 @pytest.mark.gpu
 def test_bottom_up_probe_mode_out_of_range_is_refused():
     beg, csr = gen_rmat_host(10, 8, 2)
