@@ -1161,9 +1161,11 @@ __device__ __forceinline__ int lane_owner(int ex, int t) {
 // head records, with no block barrier: each warp takes 32 words of its CTA's
 // slice at a time (one per lane), numbers their set bits with a warp scan
 // and takes the frontier vertices 64 at a time, two per lane. A lane reads
-// its vertices' head records and claims the (up to) three neighbours in
-// them; the rest of each segment (from the fourth neighbour) is expanded by
-// the warp edge-balanced over its 32 lanes, kTdIlp edges per lane in flight.
+// its vertices' head records and claims (or, on a two-phase level, marks)
+// the (up to) three neighbours in them; the rest of each segment (from the
+// fourth neighbour) is expanded by the warp edge-balanced over its 32 lanes,
+// kTdIlp edges per lane in flight, with the 64 vertices and their CSR
+// offsets in the warp's part of the window arrays.
 // Segments with more than kWarpSeg edges left go to the heavy list that is
 // expanded grid-wide, edge-balanced, after the barrier (as expand_bitmap's
 // vertices of degree above kHeavyDeg): warps do not wait for one another,
@@ -1278,9 +1280,10 @@ __device__ void expand_bitmap_heads(const Params& p, Smem& sm, Acc& acc, const Q
 // Second phase of a two-phase top-down level (after a grid barrier, when
 // every mark has landed): the new vertices are the bits of frontier L+1's
 // bitmap that are not visited. Each warp takes 32 words of its CTA's slice
-// (one per lane), sets their visited bits (one thread per word), and then
-// takes the new vertices 64 at a time, two per lane: level L+1, and the
-// frontier statistics with the degrees from their head records.
+// (one per lane), sets their visited bits (one thread per word; after blind
+// marks it also clears the bits of visited targets from frontier L+1's
+// word), and then takes the new vertices 64 at a time, two per lane: level
+// L+1, and the frontier statistics with the degrees from their head records.
 __device__ void finalize_marks(const Params& p, Acc& acc, int L, uint32_t* fbn, bool blind) {
   const long long nw = p.nwords;
   const long long G = gridDim.x, b = blockIdx.x;
